@@ -1,0 +1,354 @@
+"""egsolver_b200 -- energy-game solver for one NVIDIA B200 (sm_100a).
+
+Python mirror of the C-ABI in include/egsolver_b200.h.  Every call goes
+through the in-tree CUDA library libegsolver_b200.so; there is no CPU or
+eager-framework fallback, and a missing library raises on first use.
+
+Conventions follow the reference solver (fvella/EGSolver): player 0 is the
+file format's MAX and minimises the credit, player 1 (MIN) maximises it;
+vertices [0, num_nodes0) belong to player 0 unless an owner array is given;
+TOP (an unbounded credit) is INT32_MAX / INT64_MAX.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass, field
+from typing import Optional
+
+import numpy as np
+
+from . import _ffi
+from ._ffi import (EG_TOP32, EG_TOP64, VARIANT_AUTO, VARIANT_CTA, VARIANT_SMEM, VARIANT_THREAD,  # noqa: F401
+                   VARIANT_WARP)
+
+__all__ = ["Game", "EGError", "Stats", "solve", "ResidentGame", "generate", "read_game", "read_game_text",
+           "csr2csc", "compute_mg", "default_max_loop", "device_count", "CancelFlag", "EG_TOP32", "EG_TOP64",
+           "lib"]
+
+
+class EGError(RuntimeError):
+    """A non-OK eg_status, with the library's message."""
+
+    def __init__(self, status: int, message: str):
+        self.status = status
+        self.name = _ffi.STATUS_NAMES.get(status, str(status))
+        super().__init__(f"{self.name}: {message}")
+
+
+def lib() -> C.CDLL:
+    return _ffi.load()
+
+
+def _check(status: int) -> None:
+    if status != _ffi.EG_OK:
+        raise EGError(status, lib().eg_last_error().decode(errors="replace"))
+
+
+def _ptr(a: Optional[np.ndarray]) -> Optional[int]:
+    return None if a is None else a.ctypes.data
+
+
+@dataclass
+class Game:
+    """A game in CSR form (host arrays).
+
+    row_ptr: int64[n+1]; succ, weight: int32[m]; owner: optional uint8[n];
+    num_nodes0: split index used when owner is None; ext_id: optional
+    external names of the vertices (as read from a file).
+    """
+
+    row_ptr: np.ndarray
+    succ: np.ndarray
+    weight: np.ndarray
+    num_nodes0: int = 0
+    owner: Optional[np.ndarray] = None
+    ext_id: Optional[np.ndarray] = None
+    max_abs_weight: int = field(default=-1)
+
+    def __post_init__(self):
+        self.row_ptr = np.ascontiguousarray(self.row_ptr, dtype=np.int64)
+        self.succ = np.ascontiguousarray(self.succ, dtype=np.int32)
+        self.weight = np.ascontiguousarray(self.weight, dtype=np.int32)
+        if self.owner is not None:
+            self.owner = np.ascontiguousarray(self.owner, dtype=np.uint8)
+        if self.max_abs_weight < 0:
+            self.max_abs_weight = int(np.abs(self.weight.astype(np.int64)).max()) if self.weight.size else 0
+
+    @property
+    def num_nodes(self) -> int:
+        return int(self.row_ptr.shape[0] - 1)
+
+    @property
+    def num_edges(self) -> int:
+        return int(self.succ.shape[0])
+
+    def owners(self) -> np.ndarray:
+        if self.owner is not None:
+            return self.owner
+        o = np.ones(self.num_nodes, dtype=np.uint8)
+        o[: self.num_nodes0] = 0
+        return o
+
+    def c_struct(self) -> _ffi.EgGame:
+        g = _ffi.EgGame()
+        g.num_nodes = self.num_nodes
+        g.num_nodes0 = int(self.num_nodes0)
+        g.num_edges = self.num_edges
+        g.row_ptr = _ptr(self.row_ptr)
+        g.succ = _ptr(self.succ)
+        g.weight = _ptr(self.weight)
+        g.owner = _ptr(self.owner)
+        return g
+
+
+@dataclass
+class Stats:
+    mg: int
+    rounds: int
+    lifts: int
+    edges: int
+    num_top: int
+    solve_ms: float
+    lift_ms: float
+    kernel_launches: int
+    credit_bits: int
+    variant_small: int
+    variant_mid: int
+    variant_large: int
+    small_max_deg: int
+    large_min_deg: int
+
+    @classmethod
+    def from_c(cls, s: _ffi.EgStats) -> "Stats":
+        return cls(**s.as_dict())
+
+    @property
+    def gteps(self) -> float:
+        return self.edges / (self.solve_ms * 1e6) if self.solve_ms > 0 else 0.0
+
+
+def make_opts(credit_bits: int = 64, variant: int = VARIANT_AUTO, max_rounds: int = -1, timeout_ms: float = 0.0,
+              device: int = 0, lanes_per_vertex: int = 0, small_max_deg: int = 0, large_min_deg: int = 0,
+              keep_layout: bool = False, cancel: Optional["CancelFlag"] = None) -> _ffi.EgOpts:
+    o = _ffi.EgOpts()
+    lib().eg_opts_default(C.byref(o))
+    o.credit_bits = credit_bits
+    o.variant = variant
+    o.max_rounds = max_rounds
+    o.timeout_ms = timeout_ms
+    o.device = device
+    o.lanes_per_vertex = lanes_per_vertex
+    o.small_max_deg = small_max_deg
+    o.large_min_deg = large_min_deg
+    o.keep_layout = 1 if keep_layout else 0
+    o.cancel = cancel.ptr if cancel is not None else None
+    return o
+
+
+def solve(game: Game, credit_bits: int = 64, **kw) -> tuple[np.ndarray, Stats]:
+    """One-call solve with host buffers (eg_solve_i32 / eg_solve_i64)."""
+    opts = make_opts(credit_bits=credit_bits, **kw)
+    st = _ffi.EgStats()
+    cg = game.c_struct()
+    if credit_bits == 32:
+        out = np.zeros(game.num_nodes, dtype=np.int32)
+        _check(lib().eg_solve_i32(C.byref(cg), C.byref(opts), out.ctypes.data, C.byref(st)))
+    else:
+        out = np.zeros(game.num_nodes, dtype=np.int64)
+        _check(lib().eg_solve_i64(C.byref(cg), C.byref(opts), out.ctypes.data, C.byref(st)))
+    return out, Stats.from_c(st)
+
+
+class ResidentGame:
+    """A game kept in device memory (eg_dgame_*)."""
+
+    def __init__(self, game: Game, **kw):
+        self._h = C.c_void_p()
+        opts = make_opts(**kw)
+        cg = game.c_struct()
+        _check(lib().eg_dgame_upload(C.byref(cg), C.byref(opts), C.byref(self._h)))
+        self.num_nodes = game.num_nodes
+
+    @classmethod
+    def from_device(cls, n: int, m: int, n0: int, row_ptr_dev: int, succ_dev: int, weight_dev: int,
+                    owner_dev: Optional[int] = None, **kw) -> "ResidentGame":
+        self = cls.__new__(cls)
+        self._h = C.c_void_p()
+        g = _ffi.EgGame(n, n0, m, row_ptr_dev, succ_dev, weight_dev, owner_dev)
+        opts = make_opts(**kw)
+        _check(lib().eg_dgame_from_device(C.byref(g), C.byref(opts), C.byref(self._h)))
+        self.num_nodes = n
+        return self
+
+    def solve(self, raise_on_error: bool = True, **kw) -> tuple[int, Stats]:
+        opts = make_opts(**kw)
+        st = _ffi.EgStats()
+        status = lib().eg_dgame_solve(self._h, C.byref(opts), C.byref(st))
+        if raise_on_error:
+            _check(status)
+        return status, Stats.from_c(st)
+
+    def credits(self, bits: int = 64) -> np.ndarray:
+        if bits == 32:
+            out = np.zeros(self.num_nodes, dtype=np.int32)
+            _check(lib().eg_dgame_credits_i32(self._h, out.ctypes.data))
+        else:
+            out = np.zeros(self.num_nodes, dtype=np.int64)
+            _check(lib().eg_dgame_credits_i64(self._h, out.ctypes.data))
+        return out
+
+    def credits_device(self) -> tuple[int, int]:
+        p = C.c_void_p()
+        bits = C.c_int32()
+        _check(lib().eg_dgame_credits_device(self._h, C.byref(p), C.byref(bits)))
+        return int(p.value), int(bits.value)
+
+    @property
+    def device_bytes(self) -> int:
+        return int(lib().eg_dgame_device_bytes(self._h))
+
+    def free(self) -> None:
+        if self._h:
+            lib().eg_dgame_free(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.free()
+
+
+class CancelFlag:
+    """A flag in mapped pinned host memory that running solves poll."""
+
+    def __init__(self):
+        p = C.c_void_p()
+        _check(lib().eg_cancel_flag_alloc(C.byref(p)))
+        self.ptr = p.value
+        self._view = C.cast(p, C.POINTER(C.c_int32))
+
+    def set(self, value: int = 1) -> None:
+        self._view[0] = value
+
+    def free(self) -> None:
+        if self.ptr:
+            lib().eg_cancel_flag_free(self.ptr)
+            self.ptr = None
+
+
+def _own_to_game(og_ptr) -> Game:
+    og = og_ptr.contents
+    n = og.game.num_nodes
+    m = og.game.num_edges
+
+    def arr(addr, count, ctype, dtype):
+        if count == 0:
+            return np.zeros(0, dtype=dtype)
+        return np.ctypeslib.as_array(C.cast(addr, C.POINTER(ctype)), shape=(count,)).astype(dtype, copy=True)
+
+    g = Game(row_ptr=arr(og.row_ptr, n + 1, C.c_int64, np.int64), succ=arr(og.succ, m, C.c_int32, np.int32),
+             weight=arr(og.weight, m, C.c_int32, np.int32), num_nodes0=og.game.num_nodes0,
+             ext_id=arr(og.ext_id, n, C.c_int32, np.int32), max_abs_weight=og.max_abs_weight)
+    lib().eg_owned_game_free(og_ptr)
+    return g
+
+
+def generate(kind: int, n: int, deg: int, wmax: int, seed: int, param: int = 0) -> Game:
+    """Seeded random game (eg_generate); owner-sorted like the reference layout."""
+    out = C.POINTER(_ffi.EgOwnedGame)()
+    _check(lib().eg_generate(kind, n, deg, wmax, param, seed & (2**64 - 1), C.byref(out)))
+    return _own_to_game(out)
+
+
+def _read_opts(weight_mode: int, rnd_lo: int, rnd_hi: int, rnd_seed: int) -> _ffi.EgReadOpts:
+    return _ffi.EgReadOpts(weight_mode, rnd_lo, rnd_hi, rnd_seed)
+
+
+def read_game(path: str, weight_mode: int = 0, rnd_lo: int = -1, rnd_hi: int = 1, rnd_seed: int = 0) -> Game:
+    """Reads a game in the reference text format (gzip or plain)."""
+    out = C.POINTER(_ffi.EgOwnedGame)()
+    ro = _read_opts(weight_mode, rnd_lo, rnd_hi, rnd_seed)
+    _check(lib().eg_read_game_file(str(path).encode(), C.byref(ro), C.byref(out)))
+    return _own_to_game(out)
+
+
+def read_game_text(text: str | bytes, weight_mode: int = 0, rnd_lo: int = -1, rnd_hi: int = 1,
+                   rnd_seed: int = 0) -> Game:
+    b = text.encode() if isinstance(text, str) else text
+    out = C.POINTER(_ffi.EgOwnedGame)()
+    ro = _read_opts(weight_mode, rnd_lo, rnd_hi, rnd_seed)
+    _check(lib().eg_read_game_buffer(b, len(b), C.byref(ro), C.byref(out)))
+    return _own_to_game(out)
+
+
+def game_to_text(game: Game) -> str:
+    """The game in the reference text format, one line per vertex in
+    increasing external id: `MAX;` then `v MAX|MIN s:w,...;` (player 0 is
+    MAX), using game.ext_id as the external names when present."""
+    n = game.num_nodes
+    ext = game.ext_id if game.ext_id is not None else np.arange(n, dtype=np.int32)
+    own = game.owners()
+    order = np.argsort(ext, kind="stable")
+    lines = [f"{int(ext.max())} {game.num_edges};"]
+    rp, sc, wt = game.row_ptr, game.succ, game.weight
+    for v in order:
+        b, e = int(rp[v]), int(rp[v + 1])
+        edges = ",".join(f"{int(ext[s])}:{int(x)}" for s, x in zip(sc[b:e], wt[b:e]))
+        lines.append(f"{int(ext[v])} {'MAX' if own[v] == 0 else 'MIN'} {edges};")
+    return "\n".join(lines) + "\n"
+
+
+def write_game_text(game: Game, path: str) -> None:
+    """Writes game_to_text(game) to path, gzip-compressed when it ends in .gz."""
+    import gzip
+
+    data = game_to_text(game).encode()
+    if str(path).endswith(".gz"):
+        with gzip.open(path, "wb", compresslevel=9) as f:
+            f.write(data)
+    else:
+        with open(path, "wb") as f:
+            f.write(data)
+
+
+def csr2csc(num_rows: int, num_cols: int, row_ptr: np.ndarray, col: np.ndarray, val: np.ndarray):
+    """Device counting-sort transpose (eg_csr2csc_i32): returns (csc_ptr, csc_row, csc_val)."""
+    row_ptr = np.ascontiguousarray(row_ptr, dtype=np.int64)
+    col = np.ascontiguousarray(col, dtype=np.int32)
+    val = np.ascontiguousarray(val, dtype=np.int32)
+    nnz = col.shape[0]
+    cp = np.zeros(num_cols + 1, dtype=np.int64)
+    cr = np.zeros(max(nnz, 1), dtype=np.int32)
+    cv = np.zeros(max(nnz, 1), dtype=np.int32)
+    _check(lib().eg_csr2csc_i32(num_rows, num_cols, nnz, row_ptr.ctypes.data, col.ctypes.data, val.ctypes.data,
+                                cp.ctypes.data, cr.ctypes.data, cv.ctypes.data))
+    return cp, cr[:nnz], cv[:nnz]
+
+
+def compute_mg(game: Game, limit_bits: int = 64) -> int:
+    cg = game.c_struct()
+    mg = C.c_int64()
+    _check(lib().eg_compute_mg(C.byref(cg), limit_bits, C.byref(mg)))
+    return int(mg.value)
+
+
+def default_max_loop(m: int, n: int, mg: int, max_loop: int = -1) -> int:
+    return int(lib().eg_default_max_loop(m, n, mg, max_loop))
+
+
+def validate(game: Game) -> None:
+    cg = game.c_struct()
+    _check(lib().eg_validate(C.byref(cg)))
+
+
+def device_count() -> int:
+    c = C.c_int32()
+    status = lib().eg_device_count(C.byref(c))
+    return int(c.value) if status == _ffi.EG_OK else 0

@@ -1,0 +1,146 @@
+"""ctypes declarations of the C-ABI in include/egsolver_b200.h.
+
+The library is loaded from this package's directory; importing this module
+on a machine where it has not been built raises immediately (there is no
+fallback implementation).
+"""
+from __future__ import annotations
+
+import ctypes as C
+from pathlib import Path
+
+LIB_PATH = Path(__file__).resolve().parent / "libegsolver_b200.so"
+
+EG_OK = 0
+STATUS_NAMES = {
+    0: "EG_OK", 1: "EG_ERR_INVALID", 2: "EG_ERR_CUDA", 3: "EG_ERR_OOM", 4: "EG_ERR_TIMEOUT",
+    5: "EG_ERR_OVERFLOW", 6: "EG_ERR_LOOPCAP", 7: "EG_ERR_CANCELLED", 8: "EG_ERR_NO_DEVICE",
+    9: "EG_ERR_BUSY", 10: "EG_ERR_NOT_FOUND", 11: "EG_ERR_IO",
+}
+EG_TOP32 = 2147483647
+EG_TOP64 = 9223372036854775807
+
+VARIANT_AUTO, VARIANT_THREAD, VARIANT_WARP, VARIANT_CTA, VARIANT_SMEM = 0, 1, 2, 3, 4
+
+
+class EgGame(C.Structure):
+    _fields_ = [
+        ("num_nodes", C.c_int32),
+        ("num_nodes0", C.c_int32),
+        ("num_edges", C.c_int64),
+        ("row_ptr", C.c_void_p),
+        ("succ", C.c_void_p),
+        ("weight", C.c_void_p),
+        ("owner", C.c_void_p),
+    ]
+
+
+class EgOpts(C.Structure):
+    _fields_ = [
+        ("credit_bits", C.c_int32),
+        ("variant", C.c_int32),
+        ("small_max_deg", C.c_int32),
+        ("large_min_deg", C.c_int32),
+        ("max_rounds", C.c_int64),
+        ("timeout_ms", C.c_double),
+        ("cancel", C.c_void_p),
+        ("device", C.c_int32),
+        ("lanes_per_vertex", C.c_int32),
+        ("keep_layout", C.c_int32),
+        ("reserved", C.c_int32 * 5),
+    ]
+
+
+class EgStats(C.Structure):
+    _fields_ = [
+        ("mg", C.c_int64),
+        ("rounds", C.c_int64),
+        ("lifts", C.c_int64),
+        ("edges", C.c_int64),
+        ("num_top", C.c_int64),
+        ("solve_ms", C.c_double),
+        ("lift_ms", C.c_double),
+        ("kernel_launches", C.c_int64),
+        ("credit_bits", C.c_int32),
+        ("variant_small", C.c_int32),
+        ("variant_mid", C.c_int32),
+        ("variant_large", C.c_int32),
+        ("small_max_deg", C.c_int32),
+        ("large_min_deg", C.c_int32),
+        ("reserved", C.c_int32 * 4),
+    ]
+
+    def as_dict(self) -> dict:
+        return {k: getattr(self, k) for k, _ in self._fields_ if k != "reserved"}
+
+
+class EgOwnedGame(C.Structure):
+    _fields_ = [
+        ("game", EgGame),
+        ("row_ptr", C.c_void_p),
+        ("succ", C.c_void_p),
+        ("weight", C.c_void_p),
+        ("ext_id", C.c_void_p),
+        ("max_abs_weight", C.c_int32),
+    ]
+
+
+class EgReadOpts(C.Structure):
+    _fields_ = [
+        ("weight_mode", C.c_int32),
+        ("rnd_lo", C.c_int32),
+        ("rnd_hi", C.c_int32),
+        ("rnd_seed", C.c_uint64),
+    ]
+
+
+# every symbol the header declares, with (restype, argtypes)
+_P = C.c_void_p
+_I32, _I64 = C.c_int32, C.c_int64
+SIGNATURES = {
+    "eg_last_error": (C.c_char_p, []),
+    "eg_abi_version": (_I32, []),
+    "eg_opts_default": (None, [C.POINTER(EgOpts)]),
+    "eg_device_count": (_I32, [C.POINTER(_I32)]),
+    "eg_compute_mg": (_I32, [C.POINTER(EgGame), _I32, C.POINTER(_I64)]),
+    "eg_default_max_loop": (_I64, [_I64, _I64, _I64, _I64]),
+    "eg_validate": (_I32, [C.POINTER(EgGame)]),
+    "eg_solve_i32": (_I32, [C.POINTER(EgGame), C.POINTER(EgOpts), _P, C.POINTER(EgStats)]),
+    "eg_solve_i64": (_I32, [C.POINTER(EgGame), C.POINTER(EgOpts), _P, C.POINTER(EgStats)]),
+    "eg_dgame_upload": (_I32, [C.POINTER(EgGame), C.POINTER(EgOpts), C.POINTER(_P)]),
+    "eg_dgame_from_device": (_I32, [C.POINTER(EgGame), C.POINTER(EgOpts), C.POINTER(_P)]),
+    "eg_dgame_solve": (_I32, [_P, C.POINTER(EgOpts), C.POINTER(EgStats)]),
+    "eg_dgame_credits_i32": (_I32, [_P, _P]),
+    "eg_dgame_credits_i64": (_I32, [_P, _P]),
+    "eg_dgame_credits_device": (_I32, [_P, C.POINTER(_P), C.POINTER(_I32)]),
+    "eg_dgame_device_bytes": (_I64, [_P]),
+    "eg_dgame_free": (None, [_P]),
+    "eg_csr2csc_i32": (_I32, [_I32, _I32, _I64, _P, _P, _P, _P, _P, _P]),
+    "eg_cancel_flag_alloc": (_I32, [C.POINTER(_P)]),
+    "eg_cancel_flag_free": (None, [_P]),
+    "eg_read_game_file": (_I32, [C.c_char_p, C.POINTER(EgReadOpts), C.POINTER(C.POINTER(EgOwnedGame))]),
+    "eg_read_game_buffer": (_I32, [C.c_char_p, C.c_size_t, C.POINTER(EgReadOpts), C.POINTER(C.POINTER(EgOwnedGame))]),
+    "eg_owned_game_free": (None, [C.POINTER(EgOwnedGame)]),
+    "eg_parse_text": (_I32, [C.c_char_p, C.c_size_t, _P]),
+    "eg_read_file_bytes": (_I32, [C.c_char_p, C.POINTER(C.c_void_p), C.POINTER(C.c_size_t)]),
+    "eg_generate": (_I32, [_I32, _I32, _I32, _I32, _I32, C.c_uint64, C.POINTER(C.POINTER(EgOwnedGame))]),
+}
+
+_lib = None
+
+
+def load() -> C.CDLL:
+    """Loads the solver library (once); raises if it has not been built."""
+    global _lib
+    if _lib is None:
+        if not LIB_PATH.exists():
+            raise RuntimeError(
+                f"{LIB_PATH} is missing: build it with `python -m egsolver_b200.build` "
+                "(the solver has no CPU fallback)")
+        lib = C.CDLL(str(LIB_PATH))
+        for name, (res, args) in SIGNATURES.items():
+            fn = getattr(lib, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = lib
+    return _lib

@@ -1,0 +1,640 @@
+/*
+ * eg_api.cu -- host orchestration and the C-ABI entry points of the solver:
+ * resident games (upload, solve, credits), the one-call solve, the
+ * standalone CSR -> CSC transpose and cancel flags.
+ *
+ * The reference's GPU boundary (reference src/dev_solver.cu:81-266) keeps
+ * one packed device allocation per process and addresses it through
+ * __device__ globals set with cudaMemcpyToSymbol; here every resident game
+ * is a handle that owns its device arrays, so several games can be resident
+ * at once and no global state is shared between solves.
+ */
+#include "eg_lift.cuh"
+#include "eg_prep.cuh"
+
+#include <algorithm>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <vector>
+
+using namespace eg;
+
+#define EG_CUDA(call)                                                                                  \
+    do {                                                                                               \
+        cudaError_t _e = (call);                                                                       \
+        if (_e != cudaSuccess)                                                                         \
+            return eg_set_error(_e == cudaErrorMemoryAllocation ? EG_ERR_OOM : EG_ERR_CUDA,             \
+                                "%s failed: %s (%s:%d)", #call, cudaGetErrorString(_e), __FILE__, __LINE__); \
+    } while (0)
+
+#define EG_TRY(call)                                                                                   \
+    do {                                                                                               \
+        eg_status _s = (call);                                                                         \
+        if (_s != EG_OK) return _s;                                                                    \
+    } while (0)
+
+namespace {
+
+constexpr unsigned long long kWaitLimitNs = 5ull * 1000ull * 1000ull * 1000ull; /* 5 s per barrier wait */
+constexpr int kPrepBlock = 256;
+
+inline unsigned grid_for(long long items, int block, int cap = 148 * 32)
+{
+    long long g = (items + block - 1) / block;
+    if (g < 1) g = 1;
+    if (g > cap) g = cap;
+    return (unsigned)g;
+}
+
+inline int align32(long long x) { return (int)((x + 31) & ~31LL); }
+
+}  // namespace
+
+struct eg_dgame {
+    int device;
+    cudaStream_t st;
+    cudaEvent_t ev[4];
+    int n, n0;
+    long long m;
+    bool has_owner;
+    /* input CSR (device copy) */
+    long long *d_rowptr;
+    int *d_succ, *d_w;
+    unsigned char *d_owner;
+    /* capacities */
+    int n_pad_cap;
+    long long m_pad_cap, tmp_cap, scratch_ints;
+    /* layout of the last preprocessing */
+    bool prepared;
+    BucketBounds bb;
+    int groups[EG_MAX_CLASSES / 2];
+    ClassTable ct;
+    int n_pad, words;
+    long long m_pad;
+    int *d_perm, *d_iperm, *d_P, *d_CP, *d_CS;
+    int2 *d_E;
+    unsigned char *d_active0;
+    int *d_k0, *d_v0, *d_k1, *d_v1, *d_scratch;
+    int *d_counts;
+    unsigned long long *d_mg;
+    void *d_F, *d_out;
+    uint32_t *d_B;
+    Ctrl *d_ctrl;
+    size_t bytes;
+    long long mg;
+    int solved_bits;
+    bool solved;
+    long long launches;
+};
+
+/* ------------------------------------------------------------------ */
+/* Devices and options                                                  */
+/* ------------------------------------------------------------------ */
+
+extern "C" eg_status eg_device_count(int32_t *count)
+{
+    int n = 0;
+    *count = 0;
+    cudaError_t e = cudaGetDeviceCount(&n);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return eg_set_error(EG_ERR_NO_DEVICE, "no CUDA device: %s", cudaGetErrorString(e));
+    }
+    int ok = 0;
+    for (int d = 0; d < n; d++) {
+        int major = 0;
+        cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, d);
+        if (major == 10) ok++;
+    }
+    *count = ok;
+    return EG_OK;
+}
+
+/* Degree buckets and the lane-group size of each bucket.  AUTO: deg <= 8
+ * thread-per-vertex, 9..64 eight lanes, 65..1023 a warp, >= 1024 a CTA. */
+static void choose_layout(const eg_opts *o, BucketBounds *bb, int *groups)
+{
+    const int small = o && o->small_max_deg > 0 ? o->small_max_deg : 8;
+    const int large = o && o->large_min_deg > 0 ? o->large_min_deg : 1024;
+    const int v = o ? o->variant : EG_VARIANT_AUTO;
+    if (v == EG_VARIANT_THREAD || v == EG_VARIANT_WARP || v == EG_VARIANT_CTA) {
+        bb->nb = 1;
+        int g = 1;
+        if (v == EG_VARIANT_WARP) g = (o->lanes_per_vertex > 0) ? o->lanes_per_vertex : 32;
+        if (v == EG_VARIANT_CTA) g = EG_GROUP_CTA;
+        groups[0] = g;
+        return;
+    }
+    int nb = 0;
+    bb->upper[nb] = small;
+    groups[nb++] = 1;
+    if (small < 64 && large > 65) {
+        bb->upper[nb] = 64;
+        groups[nb++] = 8;
+    }
+    const int prev = bb->upper[nb - 1];
+    if (large - 1 > prev) {
+        bb->upper[nb] = large - 1;
+        groups[nb++] = 32;
+    }
+    groups[nb++] = EG_GROUP_CTA;
+    bb->nb = nb;
+}
+
+static eg_status check_lanes(const eg_opts *o)
+{
+    if (o && o->variant == EG_VARIANT_WARP && o->lanes_per_vertex) {
+        const int k = o->lanes_per_vertex;
+        if (k != 1 && k != 2 && k != 4 && k != 8 && k != 16 && k != 32)
+            return eg_set_error(EG_ERR_INVALID, "lanes_per_vertex must be 1, 2, 4, 8, 16 or 32 (got %d)", k);
+    }
+    if (o && o->variant == EG_VARIANT_SMEM)
+        return eg_set_error(EG_ERR_INVALID, "EG_VARIANT_SMEM is a batch-solver variant");
+    if (o && (o->variant < 0 || o->variant > EG_VARIANT_SMEM))
+        return eg_set_error(EG_ERR_INVALID, "unknown variant %d", o->variant);
+    if (o && o->credit_bits != 0 && o->credit_bits != 32 && o->credit_bits != 64)
+        return eg_set_error(EG_ERR_INVALID, "credit_bits must be 32 or 64 (got %d)", o->credit_bits);
+    return EG_OK;
+}
+
+/* ------------------------------------------------------------------ */
+/* Resident games                                                       */
+/* ------------------------------------------------------------------ */
+
+template <class P>
+static eg_status dalloc(eg_dgame *g, P **p, size_t count)
+{
+    size_t bytes = count * sizeof(P);
+    if (bytes == 0) bytes = 16;
+    cudaError_t e = cudaMalloc((void **)p, bytes);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        *p = nullptr;
+        return eg_set_error(EG_ERR_OOM, "cudaMalloc of %zu bytes failed: %s", bytes, cudaGetErrorString(e));
+    }
+    g->bytes += bytes;
+    return EG_OK;
+}
+
+extern "C" void eg_dgame_free(eg_dgame *g)
+{
+    if (!g) return;
+    int prev = 0;
+    cudaGetDevice(&prev);
+    cudaSetDevice(g->device);
+    if (g->st) cudaStreamSynchronize(g->st);
+    void *ptrs[] = {g->d_rowptr, g->d_succ, g->d_w, g->d_owner, g->d_perm, g->d_iperm, g->d_P, g->d_CP,
+                    g->d_CS, g->d_E, g->d_active0, g->d_k0, g->d_v0, g->d_k1, g->d_v1, g->d_scratch,
+                    g->d_counts, g->d_mg, g->d_F, g->d_out, g->d_B, g->d_ctrl};
+    for (void *p : ptrs)
+        if (p) cudaFree(p);
+    for (int i = 0; i < 4; i++)
+        if (g->ev[i]) cudaEventDestroy(g->ev[i]);
+    if (g->st) cudaStreamDestroy(g->st);
+    cudaSetDevice(prev);
+    free(g);
+}
+
+static eg_status dgame_alloc(const eg_game *game, const eg_opts *opts, eg_dgame **out)
+{
+    const int dev = opts ? opts->device : 0;
+    int count = 0;
+    if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0) {
+        cudaGetLastError();
+        return eg_set_error(EG_ERR_NO_DEVICE, "no CUDA device available");
+    }
+    if (dev < 0 || dev >= count) return eg_set_error(EG_ERR_INVALID, "device %d not available (%d devices)", dev, count);
+    EG_CUDA(cudaSetDevice(dev));
+    int major = 0;
+    EG_CUDA(cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, dev));
+    if (major != 10) return eg_set_error(EG_ERR_NO_DEVICE, "device %d is sm_%d0, this library is built for sm_100a", dev, major);
+    eg_dgame *g = (eg_dgame *)calloc(1, sizeof(eg_dgame));
+    if (!g) return eg_set_error(EG_ERR_OOM, "host allocation failed");
+    g->device = dev;
+    g->n = game->num_nodes;
+    g->n0 = game->num_nodes0;
+    g->m = game->num_edges;
+    g->has_owner = game->owner != nullptr;
+    g->n_pad_cap = align32(g->n) + 32 * (EG_MAX_CLASSES + 1);
+    g->m_pad_cap = g->m + g->n_pad_cap;
+    g->tmp_cap = std::max<long long>(g->m, g->n) + 1;
+    g->scratch_ints = radix_scratch_ints(g->tmp_cap) + scan_scratch_ints(g->n_pad_cap + 1) + 64;
+    eg_status s = EG_OK;
+    cudaError_t e = cudaStreamCreateWithFlags(&g->st, cudaStreamNonBlocking);
+    if (e != cudaSuccess) s = eg_set_error(EG_ERR_CUDA, "cudaStreamCreate failed: %s", cudaGetErrorString(e));
+    for (int i = 0; i < 4 && s == EG_OK; i++)
+        if (cudaEventCreate(&g->ev[i]) != cudaSuccess) s = eg_set_error(EG_ERR_CUDA, "cudaEventCreate failed");
+    const long long words = g->n_pad_cap / 32 + 2;
+    if (s == EG_OK) s = dalloc(g, &g->d_rowptr, (size_t)g->n + 1);
+    if (s == EG_OK) s = dalloc(g, &g->d_succ, (size_t)g->m);
+    if (s == EG_OK) s = dalloc(g, &g->d_w, (size_t)g->m);
+    if (s == EG_OK && g->has_owner) s = dalloc(g, &g->d_owner, (size_t)g->n);
+    if (s == EG_OK) s = dalloc(g, &g->d_perm, (size_t)g->n_pad_cap);
+    if (s == EG_OK) s = dalloc(g, &g->d_iperm, (size_t)g->n);
+    if (s == EG_OK) s = dalloc(g, &g->d_P, (size_t)g->n_pad_cap + 1);
+    if (s == EG_OK) s = dalloc(g, &g->d_CP, (size_t)g->n_pad_cap + 1);
+    if (s == EG_OK) s = dalloc(g, &g->d_CS, (size_t)g->m);
+    if (s == EG_OK) s = dalloc(g, &g->d_E, (size_t)g->m_pad_cap);
+    if (s == EG_OK) s = dalloc(g, &g->d_active0, (size_t)g->n);
+    if (s == EG_OK) s = dalloc(g, &g->d_k0, (size_t)g->tmp_cap);
+    if (s == EG_OK) s = dalloc(g, &g->d_v0, (size_t)g->tmp_cap);
+    if (s == EG_OK) s = dalloc(g, &g->d_k1, (size_t)g->tmp_cap);
+    if (s == EG_OK) s = dalloc(g, &g->d_v1, (size_t)g->tmp_cap);
+    if (s == EG_OK) s = dalloc(g, &g->d_scratch, (size_t)g->scratch_ints);
+    if (s == EG_OK) s = dalloc(g, &g->d_counts, (size_t)EG_MAX_CLASSES);
+    if (s == EG_OK) s = dalloc(g, &g->d_mg, 1);
+    if (s == EG_OK) s = dalloc(g, (int64_t **)&g->d_F, (size_t)g->n_pad_cap + 64);
+    if (s == EG_OK) s = dalloc(g, (int64_t **)&g->d_out, (size_t)g->n);
+    if (s == EG_OK) s = dalloc(g, &g->d_B, (size_t)(2 * words));
+    if (s == EG_OK) s = dalloc(g, &g->d_ctrl, 1);
+    if (s != EG_OK) {
+        eg_dgame_free(g);
+        return s;
+    }
+    *out = g;
+    return EG_OK;
+}
+
+extern "C" eg_status eg_dgame_upload(const eg_game *game, const eg_opts *opts, eg_dgame **out)
+{
+    if (!out) return eg_set_error(EG_ERR_INVALID, "out is NULL");
+    EG_TRY(eg_validate(game));
+    EG_TRY(check_lanes(opts));
+    eg_dgame *g = nullptr;
+    EG_TRY(dgame_alloc(game, opts, &g));
+    cudaError_t e = cudaMemcpyAsync(g->d_rowptr, game->row_ptr, sizeof(long long) * ((size_t)g->n + 1),
+                                    cudaMemcpyHostToDevice, g->st);
+    if (e == cudaSuccess && g->m)
+        e = cudaMemcpyAsync(g->d_succ, game->succ, sizeof(int) * (size_t)g->m, cudaMemcpyHostToDevice, g->st);
+    if (e == cudaSuccess && g->m)
+        e = cudaMemcpyAsync(g->d_w, game->weight, sizeof(int) * (size_t)g->m, cudaMemcpyHostToDevice, g->st);
+    if (e == cudaSuccess && g->has_owner)
+        e = cudaMemcpyAsync(g->d_owner, game->owner, (size_t)g->n, cudaMemcpyHostToDevice, g->st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(g->st);
+    if (e != cudaSuccess) {
+        eg_status s = eg_set_error(EG_ERR_CUDA, "upload failed: %s", cudaGetErrorString(e));
+        eg_dgame_free(g);
+        return s;
+    }
+    *out = g;
+    return EG_OK;
+}
+
+extern "C" eg_status eg_dgame_from_device(const eg_game *dev_game, const eg_opts *opts, eg_dgame **out)
+{
+    if (!dev_game || !out) return eg_set_error(EG_ERR_INVALID, "NULL argument");
+    if (dev_game->num_nodes <= 0 || dev_game->num_edges < dev_game->num_nodes ||
+        dev_game->num_edges > (int64_t)INT32_MAX - 64)
+        return eg_set_error(EG_ERR_INVALID, "game sizes out of range (n=%d, m=%lld)", dev_game->num_nodes,
+                            (long long)dev_game->num_edges);
+    EG_TRY(check_lanes(opts));
+    eg_dgame *g = nullptr;
+    EG_TRY(dgame_alloc(dev_game, opts, &g));
+    cudaError_t e = cudaMemcpyAsync(g->d_rowptr, dev_game->row_ptr, sizeof(long long) * ((size_t)g->n + 1),
+                                    cudaMemcpyDeviceToDevice, g->st);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(g->d_succ, dev_game->succ, sizeof(int) * (size_t)g->m, cudaMemcpyDeviceToDevice, g->st);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(g->d_w, dev_game->weight, sizeof(int) * (size_t)g->m, cudaMemcpyDeviceToDevice, g->st);
+    if (e == cudaSuccess && g->has_owner)
+        e = cudaMemcpyAsync(g->d_owner, dev_game->owner, (size_t)g->n, cudaMemcpyDeviceToDevice, g->st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(g->st);
+    if (e != cudaSuccess) {
+        eg_status s = eg_set_error(EG_ERR_CUDA, "device copy failed: %s", cudaGetErrorString(e));
+        eg_dgame_free(g);
+        return s;
+    }
+    *out = g;
+    return EG_OK;
+}
+
+extern "C" int64_t eg_dgame_device_bytes(const eg_dgame *g) { return g ? (int64_t)g->bytes : 0; }
+
+/* Transpose + renumbering: classify, sort classes, renumber, pack edges,
+ * counting-sort the CSC.  Leaves g->mg set (one device->host read of the
+ * class counts and MG). */
+static eg_status dgame_prepare(eg_dgame *g, const eg_opts *opts)
+{
+    cudaStream_t st = g->st;
+    const int n = g->n;
+    BucketBounds bb;
+    int groups[EG_MAX_CLASSES / 2];
+    choose_layout(opts, &bb, groups);
+    g->bb = bb;
+    memcpy(g->groups, groups, sizeof groups);
+    EG_CUDA(cudaMemsetAsync(g->d_counts, 0, sizeof(int) * EG_MAX_CLASSES, st));
+    EG_CUDA(cudaMemsetAsync(g->d_mg, 0, sizeof(unsigned long long), st));
+    k_classify<<<grid_for(n, kPrepBlock), kPrepBlock, 0, st>>>(n, g->n0, g->d_rowptr, g->d_w, g->d_owner, bb, g->d_k0,
+                                                                   g->d_v0, g->d_active0, g->d_mg, g->d_counts);
+    g->launches++;
+    int counts[EG_MAX_CLASSES];
+    unsigned long long mg = 0;
+    EG_CUDA(cudaMemcpyAsync(counts, g->d_counts, sizeof counts, cudaMemcpyDeviceToHost, st));
+    EG_CUDA(cudaMemcpyAsync(&mg, g->d_mg, sizeof mg, cudaMemcpyDeviceToHost, st));
+    int *sk, *sv;
+    const int nc = 2 * bb.nb;
+    radix_sort_pairs(g->d_k0, g->d_v0, g->d_k1, g->d_v1, n, bits_for(nc - 1), g->d_scratch, st, &sk, &sv);
+    g->launches += 3 * ((bits_for(nc - 1) + 7) / 8) + 3;
+    EG_CUDA(cudaStreamSynchronize(st));
+    g->mg = (long long)mg;
+    ClassTable ct;
+    memset(&ct, 0, sizeof ct);
+    ct.nc = nc;
+    long long pos = 0, sorted = 0;
+    for (int c = 0; c < nc; c++) {
+        ct.start[c] = (int)pos;
+        ct.count[c] = counts[c];
+        ct.sorted_begin[c] = sorted;
+        sorted += counts[c];
+        pos = align32(pos + counts[c]);
+    }
+    g->ct = ct;
+    g->n_pad = (int)pos;
+    g->words = g->n_pad / 32;
+    const int n_pad = g->n_pad;
+    EG_CUDA(cudaMemsetAsync(g->d_perm, 0xff, sizeof(int) * (size_t)n_pad, st));
+    k_build_perm<<<grid_for(n, kPrepBlock), kPrepBlock, 0, st>>>(n, sk, sv, ct, g->d_perm, g->d_iperm);
+    k_new_degree<<<grid_for(n_pad + 1, kPrepBlock), kPrepBlock, 0, st>>>(n_pad, g->d_perm, g->d_rowptr, g->d_P);
+    excl_scan(g->d_P, (long long)n_pad + 1, g->d_scratch, st);
+    EG_CUDA(cudaMemsetAsync(g->d_CP, 0, sizeof(int) * ((size_t)n_pad + 1), st));
+    k_copy_edges<<<grid_for((long long)n_pad * 32, kPrepBlock), kPrepBlock, 0, st>>>(
+        n_pad, g->d_perm, g->d_iperm, g->d_rowptr, g->d_succ, g->d_w, g->d_P, g->d_E, g->d_k0, g->d_v0, g->d_CP, ct,
+        n_pad, n_pad + 1);
+    excl_scan(g->d_CP, (long long)n_pad + 1, g->d_scratch, st);
+    radix_sort_pairs(g->d_k0, g->d_v0, g->d_k1, g->d_v1, g->m, bits_for(n_pad + 1), g->d_scratch, st, &sk, &sv);
+    EG_CUDA(cudaMemcpyAsync(g->d_CS, sv, sizeof(int) * (size_t)g->m, cudaMemcpyDeviceToDevice, st));
+    g->launches += 8 + 3 * ((bits_for(n_pad + 1) + 7) / 8) * 2;
+    EG_CUDA(cudaGetLastError());
+    g->prepared = true;
+    return EG_OK;
+}
+
+extern "C" eg_status eg_dgame_solve(eg_dgame *g, const eg_opts *opts_in, eg_stats *stats)
+{
+    if (!g) return eg_set_error(EG_ERR_INVALID, "game handle is NULL");
+    eg_opts dflt;
+    eg_opts_default(&dflt);
+    const eg_opts *opts = opts_in ? opts_in : &dflt;
+    EG_TRY(check_lanes(opts));
+    EG_CUDA(cudaSetDevice(g->device));
+    const int bits = opts->credit_bits == 32 ? 32 : 64;
+    cudaStream_t st = g->st;
+    g->launches = 0;
+    g->solved = false;
+    EG_CUDA(cudaEventRecord(g->ev[0], st));
+    if (!(opts->keep_layout && g->prepared)) EG_TRY(dgame_prepare(g, opts));
+    if (bits == 32 && g->mg > (long long)INT32_MAX)
+        return eg_set_error(EG_ERR_OVERFLOW, "MG = %lld does not fit 32-bit credits", g->mg);
+    const int n_pad = g->n_pad;
+    const int topv = n_pad;
+    launch_init_credits(bits, n_pad + 64, g->d_F, topv, st);
+    const long long wds = g->words + 2;
+    EG_CUDA(cudaMemsetAsync(g->d_B, 0, sizeof(uint32_t) * (size_t)(2 * wds), st));
+    k_init_frontier<<<grid_for(n_pad, kPrepBlock), kPrepBlock, 0, st>>>(n_pad, g->d_perm, g->d_active0, g->d_B);
+    EG_CUDA(cudaMemsetAsync(g->d_ctrl, 0, sizeof(Ctrl), st));
+    g->launches += 2;
+
+    LiftParams p;
+    memset(&p, 0, sizeof p);
+    p.P = g->d_P;
+    p.E4 = (const int4 *)g->d_E;
+    p.CP = g->d_CP;
+    p.CS = g->d_CS;
+    p.F = g->d_F;
+    p.B0 = g->d_B;
+    p.B1 = g->d_B + wds;
+    p.ctrl = g->d_ctrl;
+    p.mg = g->mg;
+    p.max_rounds = opts->max_rounds;
+    p.timeout_ns = opts->timeout_ms > 0 ? (unsigned long long)(opts->timeout_ms * 1e6) : 0ull;
+    p.wait_limit_ns = kWaitLimitNs;
+    p.cancel = nullptr;
+    if (opts->cancel) {
+        void *dp = nullptr;
+        EG_CUDA(cudaHostGetDevicePointer(&dp, (void *)opts->cancel, 0));
+        p.cancel = (const int *)dp;
+    }
+    p.n_pad = n_pad;
+    int nc = 0;
+    for (int b = g->bb.nb - 1; b >= 0; b--) {
+        for (int own = 0; own < 2; own++) {
+            const int c = b * 2 + own;
+            if (g->ct.count[c] == 0) continue;
+            LiftClass &lc = p.cls[nc++];
+            lc.word_begin = g->ct.start[c] / 32;
+            lc.word_end = (g->ct.start[c] + g->ct.count[c] + 31) / 32;
+            lc.owner = own;
+            lc.group = g->groups[b];
+            lc.grab = g->groups[b] == 1 ? 2 : 1;
+        }
+    }
+    p.nclasses = nc;
+    int grid = 0, block = 0;
+    EG_CUDA(cudaEventRecord(g->ev[1], st));
+    EG_TRY(launch_lift(p, bits, st, &grid, &block));
+    g->launches++;
+    EG_CUDA(cudaEventRecord(g->ev[2], st));
+    launch_count_top(bits, n_pad, g->d_F, &g->d_ctrl->num_top, st);
+    g->launches++;
+    EG_CUDA(cudaEventRecord(g->ev[3], st));
+    Ctrl ctrl;
+    EG_CUDA(cudaMemcpyAsync(&ctrl, g->d_ctrl, sizeof ctrl, cudaMemcpyDeviceToHost, st));
+    EG_CUDA(cudaStreamSynchronize(st));
+    float solve_ms = 0.f, lift_ms = 0.f;
+    cudaEventElapsedTime(&solve_ms, g->ev[0], g->ev[3]);
+    cudaEventElapsedTime(&lift_ms, g->ev[1], g->ev[2]);
+    g->solved_bits = bits;
+    g->solved = true;
+    if (stats) {
+        memset(stats, 0, sizeof *stats);
+        stats->mg = g->mg;
+        stats->rounds = ctrl.rounds;
+        stats->lifts = (int64_t)ctrl.lifts;
+        stats->edges = (int64_t)ctrl.edges;
+        stats->num_top = (int64_t)ctrl.num_top;
+        stats->solve_ms = solve_ms;
+        stats->lift_ms = lift_ms;
+        stats->kernel_launches = g->launches;
+        stats->credit_bits = bits;
+        stats->small_max_deg = g->bb.nb > 1 ? g->bb.upper[0] : 0;
+        stats->large_min_deg = g->bb.nb > 1 ? g->bb.upper[g->bb.nb - 2] + 1 : 0;
+        stats->variant_small = g->groups[0];
+        stats->variant_mid = g->bb.nb > 2 ? g->groups[1] : g->groups[0];
+        stats->variant_large = g->groups[g->bb.nb - 1];
+    }
+    if (ctrl.stop == EG_ERR_LOOPCAP)
+        return eg_set_error(EG_ERR_LOOPCAP, "round cap %lld reached with work left", (long long)opts->max_rounds);
+    if (ctrl.stop == EG_ERR_CANCELLED) return eg_set_error(EG_ERR_CANCELLED, "solve cancelled");
+    if (ctrl.stop == EG_ERR_TIMEOUT) {
+        if (ctrl.abort)
+            return eg_set_error(EG_ERR_TIMEOUT, "a grid barrier wait ran out after round %llu", ctrl.wait_site);
+        return eg_set_error(EG_ERR_TIMEOUT, "timeout of %.1f ms expired", opts->timeout_ms);
+    }
+    if (ctrl.stop) return eg_set_error((eg_status)ctrl.stop, "solve stopped with status %d", ctrl.stop);
+    return EG_OK;
+}
+
+template <class O>
+static eg_status dgame_credits(eg_dgame *g, O *host, int obits)
+{
+    if (!g || !host) return eg_set_error(EG_ERR_INVALID, "NULL argument");
+    if (!g->solved) return eg_set_error(EG_ERR_INVALID, "the game has no solved credits");
+    EG_CUDA(cudaSetDevice(g->device));
+    if (obits == 32 && g->solved_bits == 64 && g->mg > (long long)INT32_MAX)
+        return eg_set_error(EG_ERR_OVERFLOW, "credits do not fit 32 bits (MG = %lld)", g->mg);
+    launch_gather_out(g->solved_bits, obits, g->n, g->d_iperm, g->d_F, g->d_out, g->st);
+    EG_CUDA(cudaMemcpyAsync(host, g->d_out, sizeof(O) * (size_t)g->n, cudaMemcpyDeviceToHost, g->st));
+    EG_CUDA(cudaStreamSynchronize(g->st));
+    return EG_OK;
+}
+
+extern "C" eg_status eg_dgame_credits_i32(eg_dgame *g, int32_t *credits) { return dgame_credits<int32_t>(g, credits, 32); }
+extern "C" eg_status eg_dgame_credits_i64(eg_dgame *g, int64_t *credits) { return dgame_credits<int64_t>(g, credits, 64); }
+
+extern "C" eg_status eg_dgame_credits_device(eg_dgame *g, void **dev_ptr, int32_t *credit_bits)
+{
+    if (!g || !dev_ptr) return eg_set_error(EG_ERR_INVALID, "NULL argument");
+    if (!g->solved) return eg_set_error(EG_ERR_INVALID, "the game has no solved credits");
+    EG_CUDA(cudaSetDevice(g->device));
+    launch_gather_out(g->solved_bits, g->solved_bits, g->n, g->d_iperm, g->d_F, g->d_out, g->st);
+    EG_CUDA(cudaStreamSynchronize(g->st));
+    *dev_ptr = g->d_out;
+    if (credit_bits) *credit_bits = g->solved_bits;
+    return EG_OK;
+}
+
+/* ------------------------------------------------------------------ */
+/* One-call solve                                                       */
+/* ------------------------------------------------------------------ */
+
+template <class O>
+static eg_status solve_once(const eg_game *game, const eg_opts *opts, O *credits, eg_stats *stats, int obits)
+{
+    if (!credits) return eg_set_error(EG_ERR_INVALID, "credits is NULL");
+    eg_opts o;
+    if (opts) o = *opts;
+    else eg_opts_default(&o);
+    if (o.credit_bits == 0) o.credit_bits = obits;
+    if (obits == 32 && o.credit_bits == 64) o.credit_bits = 64; /* solve wide, narrow on output */
+    eg_dgame *g = nullptr;
+    EG_TRY(eg_dgame_upload(game, &o, &g));
+    eg_status s = eg_dgame_solve(g, &o, stats);
+    if (s == EG_OK || s == EG_ERR_LOOPCAP || s == EG_ERR_TIMEOUT || s == EG_ERR_CANCELLED) {
+        char msg[512];
+        snprintf(msg, sizeof msg, "%s", eg_last_error());
+        eg_status s2 = dgame_credits<O>(g, credits, obits);
+        if (s2 != EG_OK) s = s2;
+        else if (s != EG_OK) eg_set_error(s, "%s", msg);
+    }
+    eg_dgame_free(g);
+    return s;
+}
+
+extern "C" eg_status eg_solve_i32(const eg_game *game, const eg_opts *opts, int32_t *credits, eg_stats *stats)
+{
+    return solve_once<int32_t>(game, opts, credits, stats, 32);
+}
+
+extern "C" eg_status eg_solve_i64(const eg_game *game, const eg_opts *opts, int64_t *credits, eg_stats *stats)
+{
+    return solve_once<int64_t>(game, opts, credits, stats, 64);
+}
+
+/* ------------------------------------------------------------------ */
+/* Standalone transpose                                                 */
+/* ------------------------------------------------------------------ */
+
+extern "C" eg_status eg_csr2csc_i32(int32_t num_rows, int32_t num_cols, int64_t nnz, const int64_t *row_ptr,
+                                   const int32_t *col_idx, const int32_t *val, int64_t *csc_ptr, int32_t *csc_row,
+                                   int32_t *csc_val)
+{
+    if (num_rows < 0 || num_cols < 0 || nnz < 0 || nnz > (int64_t)INT32_MAX - 64)
+        return eg_set_error(EG_ERR_INVALID, "sizes out of range");
+    if (!row_ptr || !csc_ptr || (nnz && (!col_idx || !val || !csc_row || !csc_val)))
+        return eg_set_error(EG_ERR_INVALID, "NULL array");
+    if (row_ptr[0] != 0 || row_ptr[num_rows] != nnz)
+        return eg_set_error(EG_ERR_INVALID, "row_ptr must start at 0 and end at nnz");
+    for (int32_t r = 0; r < num_rows; r++)
+        if (row_ptr[r + 1] < row_ptr[r]) return eg_set_error(EG_ERR_INVALID, "row_ptr not monotone at row %d", r);
+    for (int64_t j = 0; j < nnz; j++)
+        if (col_idx[j] < 0 || col_idx[j] >= num_cols)
+            return eg_set_error(EG_ERR_INVALID, "column %d of entry %lld out of range", col_idx[j], (long long)j);
+    int count = 0;
+    if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0) {
+        cudaGetLastError();
+        return eg_set_error(EG_ERR_NO_DEVICE, "no CUDA device available");
+    }
+    cudaStream_t st;
+    EG_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+    const long long cap = std::max<long long>(nnz, 1);
+    long long *d_rp = nullptr, *d_cp64 = nullptr;
+    int *d_col = nullptr, *d_val = nullptr, *d_k0 = nullptr, *d_v0 = nullptr, *d_k1 = nullptr, *d_v1 = nullptr;
+    int *d_rows = nullptr, *d_cnt = nullptr, *d_orow = nullptr, *d_oval = nullptr, *d_scr = nullptr;
+    const long long scr = radix_scratch_ints(cap) + scan_scratch_ints((long long)num_cols + 1) + 64;
+    cudaError_t e = cudaSuccess;
+#define EG_MALLOC(p, n) \
+    if (e == cudaSuccess) e = cudaMalloc((void **)&p, sizeof(*p) * (size_t)(n))
+    EG_MALLOC(d_rp, (long long)num_rows + 1);
+    EG_MALLOC(d_col, cap);
+    EG_MALLOC(d_val, cap);
+    EG_MALLOC(d_k0, cap);
+    EG_MALLOC(d_v0, cap);
+    EG_MALLOC(d_k1, cap);
+    EG_MALLOC(d_v1, cap);
+    EG_MALLOC(d_rows, cap);
+    EG_MALLOC(d_orow, cap);
+    EG_MALLOC(d_oval, cap);
+    EG_MALLOC(d_cnt, (long long)num_cols + 1);
+    EG_MALLOC(d_cp64, (long long)num_cols + 1);
+    EG_MALLOC(d_scr, scr);
+#undef EG_MALLOC
+    if (e == cudaSuccess) e = cudaMemcpyAsync(d_rp, row_ptr, sizeof(long long) * ((size_t)num_rows + 1), cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess && nnz) e = cudaMemcpyAsync(d_col, col_idx, sizeof(int) * (size_t)nnz, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess && nnz) e = cudaMemcpyAsync(d_val, val, sizeof(int) * (size_t)nnz, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) e = cudaMemsetAsync(d_cnt, 0, sizeof(int) * ((size_t)num_cols + 1), st);
+    if (e == cudaSuccess) {
+        const unsigned gw = grid_for((long long)num_rows * 32, 256);
+        k_csr_expand<<<gw, 256, 0, st>>>(num_rows, d_rp, d_col, d_k0, d_v0, d_cnt);
+        k_edge_rows<<<gw, 256, 0, st>>>(num_rows, d_rp, d_rows);
+        excl_scan(d_cnt, (long long)num_cols + 1, d_scr, st);
+        int *sk, *sv;
+        radix_sort_pairs(d_k0, d_v0, d_k1, d_v1, nnz, bits_for(num_cols), d_scr, st, &sk, &sv);
+        k_csc_gather<<<grid_for(nnz, 256), 256, 0, st>>>(nnz, sv, d_rows, d_val, d_orow, d_oval);
+        k_widen<<<grid_for((long long)num_cols + 1, 256), 256, 0, st>>>((long long)num_cols + 1, d_cnt, d_cp64);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaMemcpyAsync(csc_ptr, d_cp64, sizeof(long long) * ((size_t)num_cols + 1), cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess && nnz) e = cudaMemcpyAsync(csc_row, d_orow, sizeof(int) * (size_t)nnz, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess && nnz) e = cudaMemcpyAsync(csc_val, d_oval, sizeof(int) * (size_t)nnz, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    void *ptrs[] = {d_rp, d_cp64, d_col, d_val, d_k0, d_v0, d_k1, d_v1, d_rows, d_cnt, d_orow, d_oval, d_scr};
+    for (void *ptr : ptrs)
+        if (ptr) cudaFree(ptr);
+    cudaStreamDestroy(st);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return eg_set_error(e == cudaErrorMemoryAllocation ? EG_ERR_OOM : EG_ERR_CUDA, "transpose failed: %s",
+                            cudaGetErrorString(e));
+    }
+    return EG_OK;
+}
+
+/* ------------------------------------------------------------------ */
+/* Cancel flags                                                         */
+/* ------------------------------------------------------------------ */
+
+extern "C" eg_status eg_cancel_flag_alloc(volatile int32_t **flag)
+{
+    if (!flag) return eg_set_error(EG_ERR_INVALID, "flag is NULL");
+    void *p = nullptr;
+    EG_CUDA(cudaHostAlloc(&p, 64, cudaHostAllocMapped | cudaHostAllocPortable));
+    memset(p, 0, 64);
+    *flag = (volatile int32_t *)p;
+    return EG_OK;
+}
+
+extern "C" void eg_cancel_flag_free(volatile int32_t *flag)
+{
+    if (flag) cudaFreeHost((void *)flag);
+}

@@ -1,0 +1,310 @@
+/*
+ * eg_lift.cu -- the persistent lifting kernel.
+ *
+ * One cooperative launch runs the whole least-fixed-point iteration.  Each
+ * round lifts every vertex of the current frontier bitmap and pushes the
+ * predecessors of every vertex whose credit rose into the next bitmap; a
+ * bounded grid barrier separates rounds, and the barrier's last arriver
+ * decides termination on the device (frontier empty, round cap, timeout or
+ * cancel), so there is no host round-trip per iteration.  This replaces the
+ * reference's host loop of kernel launch + thrust::remove + cudaMemset per
+ * half-iteration (reference src/dev_EG_alg.cu:307-381 and its K-lane
+ * variants, src/thrust_wrapper.cu:30-42).
+ *
+ * The lift of one vertex u is the reference kernel body
+ * (reference src/dev_EG_alg.cu:84-109): temp = min (player 0) or max
+ * (player 1) over successors w of OMINUS(f(w), wt); if f(u) < temp then
+ * f(u) = temp and every CSC predecessor is pushed.  The frontier bitmap
+ * replaces the reference's atomicCAS(flags, 0, p+1) dedup.
+ *
+ * Variants (per class of the renumbered id space, all with 128-bit loads of
+ * {succ, w, succ, w} edge pairs):
+ *   group 1       thread-per-vertex            (reference --shuffling 1)
+ *   group 2..32   G lanes per vertex, xor-shuffle min/max reduction
+ *                 (reference --shuffling G, src/dev_EG_alg.cu:397-1480)
+ *   CTA           all threads of the CTA per vertex, for high out-degree
+ *
+ * Credits are read with ld.global.cg: other SMs write them during the
+ * kernel, and an L1 line kept across a barrier would be stale.  Reads that
+ * race with a concurrent lift see the old or the new value; both are below
+ * the least fixed point and a vertex whose successor rose is pushed again,
+ * so the schedule stays a fair chaotic iteration and the result is exact.
+ */
+#include "eg_lift.cuh"
+
+namespace eg {
+
+constexpr int LIFT_BLOCK = 512;
+
+template <int OWNER, class T>
+__device__ __forceinline__ T combine(T a, T b)
+{
+    return OWNER ? (a > b ? a : b) : (a < b ? a : b);
+}
+
+template <int OWNER, class T>
+__device__ __forceinline__ T identity()
+{
+    return OWNER ? (T)0 : credit_traits<T>::top;
+}
+
+template <class T>
+__device__ __forceinline__ T shfl_xor(unsigned mask, T v, int off, int width)
+{
+    return __shfl_xor_sync(mask, v, off, width);
+}
+template <>
+__device__ __forceinline__ int64_t shfl_xor<int64_t>(unsigned mask, int64_t v, int off, int width)
+{
+    return (int64_t)__shfl_xor_sync(mask, (long long)v, off, width);
+}
+
+/* Position of the k-th (0-based) set bit of w; requires popc(w) > k. */
+__device__ __forceinline__ int nth_set_bit(uint32_t w, int k)
+{
+    int pos = 0;
+#pragma unroll
+    for (int s = 16; s > 0; s >>= 1) {
+        const uint32_t low = w & ((1u << s) - 1u);
+        const int c = __popc(low);
+        if (k >= c) {
+            k -= c;
+            w >>= s;
+            pos += s;
+        } else {
+            w = low;
+        }
+    }
+    return pos;
+}
+
+struct LiftCounters {
+    unsigned long long lifts, edges;
+    int any_new;
+};
+
+/* Lift vertex u with the G lanes of one group (gl = lane in group). */
+template <class T, int G, int OWNER>
+__device__ __forceinline__ void lift_group(const LiftParams &p, T *F, uint32_t *nxt, int u, int gl, unsigned gmask,
+                                           LiftCounters &cnt)
+{
+    const int b = __ldg(p.P + u) >> 1, e = __ldg(p.P + u + 1) >> 1;
+    T acc = identity<OWNER, T>();
+    int real = 0;
+    for (int k = b + gl; k < e; k += G) {
+        const int4 q = __ldg(p.E4 + k);
+        const T v0 = ominus<T>(ld_credit(F + q.x), q.y, p.mg);
+        const T v1 = ominus<T>(ld_credit(F + q.z), q.w, p.mg);
+        acc = combine<OWNER>(acc, combine<OWNER>(v0, v1));
+        real += 1 + (q.z < p.n_pad);
+    }
+#pragma unroll
+    for (int off = G / 2; off > 0; off >>= 1) acc = combine<OWNER>(acc, shfl_xor<T>(gmask, acc, off, G));
+    cnt.edges += (unsigned long long)real;
+    const T old = ld_credit(F + u);
+    if (old < acc) {
+        if (gl == 0) st_credit(F + u, acc);
+        const int cb = __ldg(p.CP + u), ce = __ldg(p.CP + u + 1);
+        for (int k = cb + gl; k < ce; k += G) cnt.any_new |= bitmap_push(nxt, __ldg(p.CS + k));
+    }
+    if (gl == 0) cnt.lifts++;
+}
+
+/* Warp-level processing of a class with G lanes per vertex: warps grab
+ * frontier words dynamically; within a word, group g takes the g-th set bit. */
+template <class T, int G, int OWNER>
+__device__ __noinline__ void warp_class(const LiftParams &p, const LiftClass &lc, T *F, uint32_t *cur, uint32_t *nxt,
+                                        int *ctr, LiftCounters &cnt)
+{
+    const int lane = threadIdx.x & 31;
+    const int nwords = lc.word_end - lc.word_begin;
+    constexpr int NG = 32 / G;
+    const int grp = lane / G, gl = lane % G;
+    const unsigned gmask = (G == 32) ? 0xffffffffu : (((1u << G) - 1u) << (grp * G));
+    for (;;) {
+        int w0 = 0;
+        if (lane == 0) w0 = atomicAdd(ctr, lc.grab);
+        w0 = __shfl_sync(0xffffffffu, w0, 0);
+        if (w0 >= nwords) break;
+        const int w1 = min(w0 + lc.grab, nwords);
+        for (int wi = w0; wi < w1; wi++) {
+            const int gw = lc.word_begin + wi;
+            uint32_t word = 0;
+            if (lane == 0) {
+                word = __ldcg(cur + gw);
+                if (word) __stcg(cur + gw, 0u);
+            }
+            word = __shfl_sync(0xffffffffu, word, 0);
+            const int base_u = gw << 5;
+            if (G == 1) {
+                if ((word >> lane) & 1u) lift_group<T, 1, OWNER>(p, F, nxt, base_u + lane, 0, 0u, cnt);
+            } else {
+                while (word) {
+                    const int c = __popc(word);
+                    if (grp < c) lift_group<T, G, OWNER>(p, F, nxt, base_u + nth_set_bit(word, grp), gl, gmask, cnt);
+                    if (c <= NG) {
+                        word = 0;
+                    } else {
+                        const int last = nth_set_bit(word, NG - 1);
+                        word &= ~((2u << last) - 1u);
+                    }
+                }
+            }
+        }
+    }
+}
+
+/* CTA-level processing: the whole CTA lifts one vertex at a time. */
+template <class T, int OWNER>
+__device__ __noinline__ void cta_class(const LiftParams &p, const LiftClass &lc, T *F, uint32_t *cur, uint32_t *nxt,
+                                       int *ctr, LiftCounters &cnt)
+{
+    __shared__ int s_w;
+    __shared__ uint32_t s_word;
+    __shared__ T s_red[LIFT_BLOCK / 32];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    const int nwords = lc.word_end - lc.word_begin;
+    for (;;) {
+        if (threadIdx.x == 0) {
+            const int w = atomicAdd(ctr, 1);
+            uint32_t word = 0;
+            if (w < nwords) {
+                word = __ldcg(cur + lc.word_begin + w);
+                if (word) __stcg(cur + lc.word_begin + w, 0u);
+            }
+            s_w = w;
+            s_word = word;
+        }
+        __syncthreads();
+        const int w = s_w;
+        uint32_t word = s_word;
+        __syncthreads();
+        if (w >= nwords) break;
+        while (word) {
+            const int bit = __ffs(word) - 1;
+            word &= word - 1u;
+            const int u = ((lc.word_begin + w) << 5) + bit;
+            const int b = __ldg(p.P + u) >> 1, e = __ldg(p.P + u + 1) >> 1;
+            T acc = identity<OWNER, T>();
+            int real = 0;
+            for (int k = b + threadIdx.x; k < e; k += LIFT_BLOCK) {
+                const int4 q = __ldg(p.E4 + k);
+                const T v0 = ominus<T>(ld_credit(F + q.x), q.y, p.mg);
+                const T v1 = ominus<T>(ld_credit(F + q.z), q.w, p.mg);
+                acc = combine<OWNER>(acc, combine<OWNER>(v0, v1));
+                real += 1 + (q.z < p.n_pad);
+            }
+            cnt.edges += (unsigned long long)real;
+#pragma unroll
+            for (int off = 16; off > 0; off >>= 1) acc = combine<OWNER>(acc, shfl_xor<T>(0xffffffffu, acc, off, 32));
+            if (lane == 0) s_red[wid] = acc;
+            __syncthreads();
+            if (wid == 0) {
+                T x = lane < LIFT_BLOCK / 32 ? s_red[lane] : identity<OWNER, T>();
+#pragma unroll
+                for (int off = 16; off > 0; off >>= 1) x = combine<OWNER>(x, shfl_xor<T>(0xffffffffu, x, off, 32));
+                if (lane == 0) s_red[0] = x;
+            }
+            __syncthreads();
+            acc = s_red[0];
+            const T old = ld_credit(F + u);
+            if (old < acc) {
+                if (threadIdx.x == 0) st_credit(F + u, acc);
+                const int cb = __ldg(p.CP + u), ce = __ldg(p.CP + u + 1);
+                for (int k = cb + threadIdx.x; k < ce; k += LIFT_BLOCK) cnt.any_new |= bitmap_push(nxt, __ldg(p.CS + k));
+            }
+            if (threadIdx.x == 0) cnt.lifts++;
+            __syncthreads();
+        }
+    }
+}
+
+template <class T, int OWNER>
+__device__ __forceinline__ void run_class(const LiftParams &p, const LiftClass &lc, T *F, uint32_t *cur, uint32_t *nxt,
+                                          int *ctr, LiftCounters &cnt)
+{
+    switch (lc.group) {
+    case EG_GROUP_CTA: cta_class<T, OWNER>(p, lc, F, cur, nxt, ctr, cnt); break;
+    case 1: warp_class<T, 1, OWNER>(p, lc, F, cur, nxt, ctr, cnt); break;
+    case 2: warp_class<T, 2, OWNER>(p, lc, F, cur, nxt, ctr, cnt); break;
+    case 4: warp_class<T, 4, OWNER>(p, lc, F, cur, nxt, ctr, cnt); break;
+    case 8: warp_class<T, 8, OWNER>(p, lc, F, cur, nxt, ctr, cnt); break;
+    case 16: warp_class<T, 16, OWNER>(p, lc, F, cur, nxt, ctr, cnt); break;
+    default: warp_class<T, 32, OWNER>(p, lc, F, cur, nxt, ctr, cnt); break;
+    }
+}
+
+template <class T>
+__global__ void __launch_bounds__(LIFT_BLOCK, 2) k_lift(const __grid_constant__ LiftParams p)
+{
+    Ctrl *c = p.ctrl;
+    T *F = (T *)p.F;
+    LiftCounters cnt = {0ull, 0ull, 0};
+    if (blockIdx.x == 0 && threadIdx.x == 0) c->t_start = globaltimer_ns();
+    for (long long round = 0;; round++) {
+        uint32_t *cur = (round & 1) ? p.B1 : p.B0;
+        uint32_t *nxt = (round & 1) ? p.B0 : p.B1;
+        int *ctr = c->ctr[round & 1];
+        cnt.any_new = 0;
+        for (int ci = 0; ci < p.nclasses; ci++) {
+            const LiftClass &lc = p.cls[ci];
+            if (lc.owner) run_class<T, 1>(p, lc, F, cur, nxt, ctr + ci, cnt);
+            else run_class<T, 0>(p, lc, F, cur, nxt, ctr + ci, cnt);
+        }
+        if (__syncthreads_or(cnt.any_new) && threadIdx.x == 0) c->flag[(round + 1) & 1] = 1;
+        const bool ok = grid_barrier(c, p.wait_limit_ns, [&]() {
+            /* last arriver of round `round`: clear this parity's counters
+             * and flag, then decide whether the solve goes on */
+            for (int ci = 0; ci < EG_MAX_CLASSES; ci++) c->ctr[round & 1][ci] = 0;
+            c->flag[round & 1] = 0;
+            c->rounds = round + 1;
+            if (ld_volatile(&c->flag[(round + 1) & 1])) {
+                if (p.max_rounds >= 0 && round + 1 >= p.max_rounds) {
+                    c->stop = (int)EG_ERR_LOOPCAP;
+                } else if (p.timeout_ns && globaltimer_ns() - c->t_start > p.timeout_ns) {
+                    c->stop = (int)EG_ERR_TIMEOUT;
+                } else if (p.cancel && (round & 63) == 0 && ld_volatile(p.cancel)) {
+                    c->stop = (int)EG_ERR_CANCELLED;
+                }
+            }
+        });
+        if (!ok) break;
+        if (ld_volatile(&c->stop)) break;
+        if (!ld_volatile(&c->flag[(round + 1) & 1])) break;
+    }
+    /* statistics */
+    unsigned long long l = cnt.lifts, e = cnt.edges;
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) {
+        l += __shfl_xor_sync(0xffffffffu, l, off);
+        e += __shfl_xor_sync(0xffffffffu, e, off);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        atomicAdd(&c->lifts, l);
+        atomicAdd(&c->edges, e);
+    }
+}
+
+eg_status launch_lift(const LiftParams &p, int credit_bits, cudaStream_t st, int *grid, int *block)
+{
+    int dev = 0;
+    cudaGetDevice(&dev);
+    int sms = 0;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const void *fn = credit_bits == 32 ? (const void *)k_lift<int32_t> : (const void *)k_lift<int64_t>;
+    int per_sm = 0;
+    cudaError_t err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, LIFT_BLOCK, 0);
+    if (err != cudaSuccess || per_sm < 1)
+        return eg_set_error(EG_ERR_CUDA, "occupancy query for the lifting kernel failed: %s",
+                            cudaGetErrorString(err));
+    const int g = sms * per_sm;
+    void *args[] = {(void *)&p};
+    err = cudaLaunchCooperativeKernel(fn, dim3(g), dim3(LIFT_BLOCK), args, 0, st);
+    if (err != cudaSuccess)
+        return eg_set_error(EG_ERR_CUDA, "cooperative launch of the lifting kernel failed: %s", cudaGetErrorString(err));
+    *grid = g;
+    *block = LIFT_BLOCK;
+    return EG_OK;
+}
+
+}  // namespace eg

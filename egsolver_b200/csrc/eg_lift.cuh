@@ -1,0 +1,46 @@
+/*
+ * eg_lift.cuh -- parameters of the persistent lifting kernel.
+ */
+#ifndef EG_LIFT_CUH
+#define EG_LIFT_CUH
+
+#include "eg_device.cuh"
+
+namespace eg {
+
+/* Lane-group sizes of the lifting variants; EG_GROUP_CTA lifts one vertex
+ * with the whole CTA. */
+enum { EG_GROUP_CTA = 0 };
+
+struct LiftClass {
+    int word_begin, word_end;  /* frontier words of the class              */
+    int owner;                 /* 0: min (player 0), 1: max (player 1)      */
+    int group;                 /* lanes per vertex: 1..32, or EG_GROUP_CTA  */
+    int grab;                  /* frontier words taken per work grab        */
+};
+
+struct LiftParams {
+    const int *P;              /* padded row offsets, n_pad + 1             */
+    const int4 *E4;            /* edge pairs {succ, w, succ, w}             */
+    const int *CP;             /* predecessor offsets, n_pad + 1            */
+    const int *CS;             /* predecessor ids                           */
+    void *F;                   /* credits (int32 or int64), n_pad + 64      */
+    uint32_t *B0, *B1;         /* frontier bitmaps                          */
+    Ctrl *ctrl;
+    long long mg;
+    long long max_rounds;      /* < 0: no cap                               */
+    unsigned long long timeout_ns;     /* 0: none                           */
+    unsigned long long wait_limit_ns;  /* bound of every barrier wait       */
+    const int *cancel;         /* device view of a mapped host flag, or 0   */
+    int n_pad;                 /* ids >= n_pad are the padding sentinels    */
+    int nclasses;
+    LiftClass cls[EG_MAX_CLASSES];
+};
+
+/* Cooperative launch of the persistent lifting kernel on `st`; *grid gets
+ * the number of CTAs used. */
+eg_status launch_lift(const LiftParams &p, int credit_bits, cudaStream_t st, int *grid, int *block);
+
+}  // namespace eg
+
+#endif

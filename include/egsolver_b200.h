@@ -1,0 +1,278 @@
+/*
+ * egsolver_b200.h -- C-ABI of the B200 energy-game solver.
+ *
+ * An energy game is a directed graph whose vertices belong to player 0 or
+ * player 1 and whose edges carry integer weights.  For every vertex v the
+ * solver computes the minimal initial credit f(v): the least value that the
+ * lifting operator of Brim, Chaloupka, Doyen, Gentilini and Raskin reaches
+ * from f = 0,
+ *
+ *     f(v) = min_{(v,w)} OMINUS(f(w), wt(v,w))   if v belongs to player 0
+ *     f(v) = max_{(v,w)} OMINUS(f(w), wt(v,w))   if v belongs to player 1
+ *     OMINUS(a, b) = (a < TOP && a - b <= MG) ? max(0, a - b) : TOP
+ *     MG = sum_v max(0, -min_{(v,w)} wt(v,w))
+ *
+ * TOP marks a vertex from which player 0 cannot keep the energy non-negative
+ * with any finite credit.  Player 0 is the owner the reference text format
+ * calls MAX (reference: src/the_parser.y:87), player 1 is MIN (:88); the
+ * operator is the macro OMINUS of reference src/common.h:270-272.
+ *
+ * Every result is bit-exact against the reference CPU solver
+ * (reference src/cpu_solver.c:190-333): the least fixed point is unique, so
+ * any fair schedule of lifts reaches the same f.
+ *
+ * All entry points return an eg_status; none calls exit().  Buffers are owned
+ * by the caller unless an entry point says otherwise.  No torch type appears
+ * in any signature.
+ */
+#ifndef EGSOLVER_B200_H
+#define EGSOLVER_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define EG_ABI_VERSION 1
+
+/* TOP as stored in 32-bit credits: INT_MAX, the value the reference prints
+ * for an unbounded credit (reference src/common.h:271, src/egsolver.c:103). */
+#define EG_TOP32 ((int32_t)2147483647)
+/* TOP as stored in 64-bit credits. */
+#define EG_TOP64 ((int64_t)9223372036854775807LL)
+
+typedef enum eg_status {
+    EG_OK = 0,
+    EG_ERR_INVALID = 1,      /* malformed game or option (message in eg_last_error) */
+    EG_ERR_CUDA = 2,         /* a CUDA call failed (message in eg_last_error)       */
+    EG_ERR_OOM = 3,          /* device or host allocation failed / admission denied */
+    EG_ERR_TIMEOUT = 4,      /* opts.timeout_ms expired or a device wait ran out    */
+    EG_ERR_OVERFLOW = 5,     /* MG does not fit the chosen credit width             */
+    EG_ERR_LOOPCAP = 6,      /* opts.max_rounds reached with work left (partial f)  */
+    EG_ERR_CANCELLED = 7,    /* the cancel flag was raised                          */
+    EG_ERR_NO_DEVICE = 8,    /* no CUDA device, or not an sm_100 device             */
+    EG_ERR_BUSY = 9,         /* serving queue full                                  */
+    EG_ERR_NOT_FOUND = 10,   /* unknown request / game handle                       */
+    EG_ERR_IO = 11           /* file could not be read or parsed                    */
+} eg_status;
+
+/* Kernel variants for the lifting step, per out-degree bucket.  The names
+ * follow the reference's kinds of parallelism (reference src/common.h:195-202,
+ * --shuffling K): one thread per vertex, a group of lanes per vertex with
+ * shuffle min/max reductions, and (new) one CTA per vertex. */
+typedef enum eg_variant {
+    EG_VARIANT_AUTO = 0,     /* autotuned per degree bucket                          */
+    EG_VARIANT_THREAD = 1,   /* thread-per-vertex  (reference --shuffling 1)         */
+    EG_VARIANT_WARP = 2,     /* warp-per-vertex, __shfl reductions (--shuffling 32) */
+    EG_VARIANT_CTA = 3,      /* CTA-per-vertex for high out-degree                   */
+    EG_VARIANT_SMEM = 4      /* whole game resident in one CTA's shared memory       */
+} eg_variant;
+
+/* A game in compressed sparse row form, vertices 0..num_nodes-1.
+ * Owners are given either by a split index (the reference layout:
+ * vertices [0, num_nodes0) belong to player 0, the rest to player 1;
+ * reference src/egsolver.c:253-281, counter_nodi0) when owner == NULL, or by
+ * a per-vertex owner array (0 or 1) when owner != NULL.  Every vertex must
+ * have at least one successor, as in the reference. */
+typedef struct eg_game {
+    int32_t num_nodes;
+    int32_t num_nodes0;          /* used only when owner == NULL           */
+    int64_t num_edges;
+    const int64_t *row_ptr;      /* num_nodes + 1 offsets into succ/weight */
+    const int32_t *succ;         /* num_edges successor ids                */
+    const int32_t *weight;       /* num_edges edge weights                 */
+    const uint8_t *owner;        /* optional, num_nodes entries            */
+} eg_game;
+
+typedef struct eg_opts {
+    int32_t credit_bits;         /* 32, 64, or 0 = 64                                 */
+    int32_t variant;             /* eg_variant; AUTO picks per bucket                 */
+    int32_t small_max_deg;       /* bucket bound: deg <= this -> small bucket (0=auto) */
+    int32_t large_min_deg;       /* bucket bound: deg >= this -> large bucket (0=auto) */
+    int64_t max_rounds;          /* <0: no cap (reference default n*m*MG+1)           */
+    double  timeout_ms;          /* <=0: none; checked on the device every round      */
+    volatile int32_t *cancel;    /* optional flag from eg_cancel_flag_alloc()         */
+    int32_t device;              /* CUDA device ordinal                                */
+    int32_t lanes_per_vertex;    /* with EG_VARIANT_WARP: 2,4,8,16 or 32 lanes per
+                                    vertex (reference --shuffling K); 0 means 32       */
+    int32_t keep_layout;         /* non-zero: reuse the transpose/renumbering of the
+                                    previous solve of the same resident game           */
+    int32_t reserved[5];
+} eg_opts;
+
+typedef struct eg_stats {
+    int64_t mg;                  /* MG of the game (reference MG_pesi)                */
+    int64_t rounds;              /* synchronous rounds run on the device              */
+    int64_t lifts;               /* vertices lifted (reference processedNodes)        */
+    int64_t edges;               /* sum of out-degrees of lifted vertices             */
+    int64_t num_top;             /* vertices whose credit is TOP                       */
+    double  solve_ms;            /* device time of the solve (transpose included)    */
+    double  lift_ms;             /* device time of the lifting loop alone            */
+    int64_t kernel_launches;     /* kernels launched by the solve                     */
+    int32_t credit_bits;         /* width actually used                               */
+    int32_t variant_small, variant_mid, variant_large; /* variants used per bucket   */
+    int32_t small_max_deg, large_min_deg;               /* bucket bounds used         */
+    int32_t reserved[4];
+} eg_stats;
+
+/* ------------------------------------------------------------------ */
+/* Library and device                                                   */
+/* ------------------------------------------------------------------ */
+
+/* Message of the last failing call on this thread (never NULL). */
+const char *eg_last_error(void);
+/* EG_ABI_VERSION of the loaded library. */
+int32_t eg_abi_version(void);
+/* Fills opts with defaults: 64-bit credits, autotuned variants, no cap. */
+void eg_opts_default(eg_opts *opts);
+/* Number of usable sm_100 devices (0 when none). */
+eg_status eg_device_count(int32_t *count);
+
+/* ------------------------------------------------------------------ */
+/* Host-side helpers that mirror the reference's preprocessing          */
+/* ------------------------------------------------------------------ */
+
+/* MG = sum over vertices of max(0, -(min out-weight)).  Mirrors
+ * reference src/egsolver.c:283-304; returns EG_ERR_OVERFLOW when
+ * limit_bits == 32 and the sum exceeds INT_MAX, like the reference's
+ * "too high weights" exit. */
+eg_status eg_compute_mg(const eg_game *game, int32_t limit_bits, int64_t *mg);
+
+/* Round cap used by the reference when none is given:
+ * n*m*MG+1, or LONG_MAX-1 on overflow (reference src/egsolver.c:64-90). */
+int64_t eg_default_max_loop(int64_t num_edges, int64_t num_nodes, int64_t mg, int64_t max_loop);
+
+/* Checks the CSR: offsets monotone, ids in range, no vertex without a
+ * successor, owner values 0/1. */
+eg_status eg_validate(const eg_game *game);
+
+/* ------------------------------------------------------------------ */
+/* One-call solve (host buffers in, host buffers out)                   */
+/* ------------------------------------------------------------------ */
+
+/* Copies the game to the device, transposes it, lifts to the least fixed
+ * point and copies the credits back.  Replaces the reference's
+ * copia_dati_su_device + gpu_solver + result copy
+ * (reference src/dev_solver.cu:81-139, :142-149).  credits has num_nodes
+ * entries; TOP is EG_TOP32 / EG_TOP64. */
+eg_status eg_solve_i32(const eg_game *game, const eg_opts *opts, int32_t *credits, eg_stats *stats);
+eg_status eg_solve_i64(const eg_game *game, const eg_opts *opts, int64_t *credits, eg_stats *stats);
+
+/* ------------------------------------------------------------------ */
+/* Device-resident games (inputs already in HBM)                        */
+/* ------------------------------------------------------------------ */
+
+typedef struct eg_dgame eg_dgame;
+
+/* Uploads a host game: allocates device memory for its CSR and all solve
+ * state.  The handle keeps them resident until eg_dgame_free. */
+eg_status eg_dgame_upload(const eg_game *game, const eg_opts *opts, eg_dgame **out);
+/* Same, from a CSR that is already in device memory (pointers are device
+ * pointers; owner may be NULL).  The arrays are copied, not adopted. */
+eg_status eg_dgame_from_device(const eg_game *dev_game, const eg_opts *opts, eg_dgame **out);
+/* Solves a resident game from f = 0: transpose, bucket, init, lift.  The
+ * credits stay on the device; stats are filled. */
+eg_status eg_dgame_solve(eg_dgame *g, const eg_opts *opts, eg_stats *stats);
+/* Copies the credits of the last solve to the host (original vertex ids). */
+eg_status eg_dgame_credits_i32(eg_dgame *g, int32_t *credits);
+eg_status eg_dgame_credits_i64(eg_dgame *g, int64_t *credits);
+/* Device pointer to the credits of the last solve, in original vertex order
+ * (int32 or int64 as solved); valid until the next solve or free. */
+eg_status eg_dgame_credits_device(eg_dgame *g, void **dev_ptr, int32_t *credit_bits);
+/* Device bytes held by the handle. */
+int64_t eg_dgame_device_bytes(const eg_dgame *g);
+void eg_dgame_free(eg_dgame *g);
+
+/* ------------------------------------------------------------------ */
+/* CSR -> CSC transpose (the reference's csr2csc / host_csr2csc)        */
+/* ------------------------------------------------------------------ */
+
+/* Deterministic counting-sort transpose on the device of a host CSR:
+ * csc_ptr (n+1), csc_src (m), csc_val (m) come out array-equal to the
+ * reference's host_csr2csc (reference src/host_csr2csc.c:15-46): within
+ * each column the entries keep their source order.  Replaces
+ * cusparseScsr2csc (reference src/csr2csc.cu:54-66). */
+eg_status eg_csr2csc_i32(int32_t num_rows, int32_t num_cols, int64_t nnz,
+                         const int64_t *row_ptr, const int32_t *col_idx, const int32_t *val,
+                         int64_t *csc_ptr, int32_t *csc_row, int32_t *csc_val);
+
+/* ------------------------------------------------------------------ */
+/* Cancellation                                                         */
+/* ------------------------------------------------------------------ */
+
+/* Allocates a flag in mapped pinned host memory that a running solve polls
+ * once per round; writing a non-zero value makes the solve stop with
+ * EG_ERR_CANCELLED. */
+eg_status eg_cancel_flag_alloc(volatile int32_t **flag);
+void eg_cancel_flag_free(volatile int32_t *flag);
+
+/* ------------------------------------------------------------------ */
+/* Game reader (reference text format, optionally gzip-compressed)      */
+/* ------------------------------------------------------------------ */
+
+/* An owned game as read from a file: CSR in owner-sorted internal order
+ * (player 0 first, as reference src/egsolver.c:107-281 builds it), plus
+ * the external name of every internal vertex. */
+typedef struct eg_owned_game {
+    eg_game game;                /* pointers below, owner == NULL          */
+    int64_t *row_ptr;
+    int32_t *succ;
+    int32_t *weight;
+    int32_t *ext_id;             /* ext_id[internal] = id in the file      */
+    int32_t max_abs_weight;      /* reference max_pesi                     */
+} eg_owned_game;
+
+/* Weight rewrite modes of the reader (reference src/the_parser.y:324-327,
+ * --unit-weights / --rnd-weights). */
+typedef struct eg_read_opts {
+    int32_t weight_mode;         /* 0 keep, 1 unit, 3 random in [lo, hi]   */
+    int32_t rnd_lo, rnd_hi;
+    uint64_t rnd_seed;
+} eg_read_opts;
+
+/* Parses "MAX [EDGES];" then "v MAX|MIN s:w,...,s:w ["name"];" lines
+ * (reference src/the_lex.l:33-52, src/the_parser.y:121-160). */
+eg_status eg_read_game_file(const char *path, const eg_read_opts *ropts, eg_owned_game **out);
+eg_status eg_read_game_buffer(const char *text, size_t len, const eg_read_opts *ropts, eg_owned_game **out);
+void eg_owned_game_free(eg_owned_game *g);
+
+/* Streaming form of the same parser: each grammar action calls back, in the
+ * order of the reference's parser actions (reference src/the_parser.y:186-301:
+ * header, per line node + edges + node_end, footer).  owner is 0 for MAX and
+ * 1 for MIN; name points into the text without its quotes (NULL if absent).
+ * A callback returns 0 to continue or an eg_status to stop. */
+typedef struct eg_parse_cb {
+    void *ctx;
+    int (*header)(void *ctx, int32_t max_id);
+    int (*node)(void *ctx, int32_t id, int32_t owner, int line);
+    int (*edge)(void *ctx, int32_t succ, int32_t weight, int line);
+    int (*node_end)(void *ctx, const char *name, size_t name_len);
+    int (*footer)(void *ctx);
+} eg_parse_cb;
+eg_status eg_parse_text(const char *text, size_t len, const eg_parse_cb *cb);
+/* Reads a whole file, gunzipping it when compressed; *buf is malloc'd. */
+eg_status eg_read_file_bytes(const char *path, char **buf, size_t *len);
+
+/* ------------------------------------------------------------------ */
+/* Seeded generators for the benchmark workloads                        */
+/* ------------------------------------------------------------------ */
+
+/* Generates a random game in owner-sorted order.
+ *   kind 1: n vertices, exactly `deg` distinct successors (no self-loops),
+ *           weights uniform in [-wmax, wmax]
+ *   kind 2: out-degree floor of a continuous power law x^-2 on
+ *           [1, deg+1) clipped to [1, deg], distinct, no self-loops
+ *   kind 3: complete digraph without self-loops
+ *   kind 4: out-degree uniform in {deg_lo..deg} (deg_lo = `param`)
+ *   kind 5: out-degree 1 + geometric with mean `param` - 1 (mean `param`)
+ * Owners are independent fair coins.  Deterministic in `seed`. */
+eg_status eg_generate(int32_t kind, int32_t n, int32_t deg, int32_t wmax, int32_t param,
+                      uint64_t seed, eg_owned_game **out);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* EGSOLVER_B200_H */

@@ -1,0 +1,62 @@
+"""Regenerates the golden fixtures of this directory from the reference tree.
+
+    python tests/golden/make_golden.py [REFERENCE_TREE]
+
+Reads, from the reference project (fvella/EGSolver):
+  script/clique_500_cp4.txt.gz   2000-vertex game (1,746,500 edges, weights +-1)
+  script/sol.txt                 its solution as printed by the reference
+                                 (`egsolver --input clique_500_cp4.txt.gz --eg0
+                                 --cpu`, lines 43-2043 "ext)<TAB>credit")
+  script/multi/eg_fig2.txt       5-vertex example game (no expected output
+                                 ships with it)
+
+and writes:
+  clique_500_cp4.txt.gz   the same game re-serialised by this library's
+                          writer (same vertices, owners, edge order, weights)
+  clique_500_cp4.sol      "ext credit" per vertex, from sol.txt
+  eg_fig2.txt             the example game, re-serialised
+  eg_fig2.sol             its credits, [0, 3, TOP, 0, TOP] for vertices 0..4:
+                          derived by hand and confirmed by running the
+                          reference's own driver (oracle/_ref/egsolver --cpu)
+
+The fixtures are committed; the GPU box has no reference tree.
+"""
+from __future__ import annotations
+
+import sys
+from pathlib import Path
+
+HERE = Path(__file__).resolve().parent
+sys.path.insert(0, str(HERE.parents[1]))
+
+import egsolver_b200 as eg  # noqa: E402
+
+
+def parse_solution(text: str) -> list[tuple[int, int]]:
+    out = []
+    in_sol = False
+    for line in text.splitlines():
+        if line.startswith("Solution:"):
+            in_sol = True
+            continue
+        if in_sol and ")" in line and line.split(")")[0].strip().isdigit():
+            k, v = line.split(")")
+            out.append((int(k), int(v.strip())))
+    return out
+
+
+def main(ref: Path) -> None:
+    game = eg.read_game(str(ref / "script" / "clique_500_cp4.txt.gz"))
+    eg.write_game_text(game, str(HERE / "clique_500_cp4.txt.gz"))
+    sol = parse_solution((ref / "script" / "sol.txt").read_text())
+    assert len(sol) == 2000, len(sol)
+    (HERE / "clique_500_cp4.sol").write_text("".join(f"{k} {v}\n" for k, v in sorted(sol)))
+    fig = eg.read_game(str(ref / "script" / "multi" / "eg_fig2.txt"))
+    (HERE / "eg_fig2.txt").write_text(eg.game_to_text(fig))
+    top = 2147483647
+    (HERE / "eg_fig2.sol").write_text("".join(f"{k} {v}\n" for k, v in enumerate([0, 3, top, 0, top])))
+    print("wrote fixtures to", HERE)
+
+
+if __name__ == "__main__":
+    main(Path(sys.argv[1]) if len(sys.argv) > 1 else Path("/root/reference"))
