@@ -1,0 +1,372 @@
+#!/usr/bin/env python
+"""Benchmark of the energy-game solve on B200: GTEPS of the full solve.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Workload (default): one game of n = 2^20 vertices, owners 50/50, out-degree
+floor of a continuous x^-2 power law on [1, 4097) (mean 7.9, m = 8.28M),
+successors uniform without self-loops or duplicates, weights uniform in
+[-1000, 1000], 64-bit credits; seeded (seed 0xE6 + 2), synthetic.
+
+A step is one complete solve from f = 0: transpose and renumbering,
+initial frontier, the persistent lifting kernel until the least fixed point.
+  value  GTEPS = out-edges scanned by lifts / device time of the solve, with
+         the game resident in HBM; device time from CUDA events on the
+         solver's stream; L2 flushed (256 MB write) before every step
+  e2e    the same metric through the one-call public API eg_solve_i64 with
+         pinned host buffers: allocation, host->device copy of the CSR, solve,
+         device->host copy of the credits, per step (wall clock)
+  roofline   the lifting kernel's algorithmic bytes / its event time, against
+         the measured HBM copy bandwidth
+  cpu_baseline   the reference's own EG_cpu_solver (oracle/_ref, compiled
+         unmodified; serial worklist, 1 core) on a bounded sample of the same
+         game: its first P worklist pops (reference --eg P)
+
+With N > 1 (torchrun), every rank solves its own replica on its own GPU (the
+single-game solve does not shard); value = edges of all ranks / max time.
+
+--impl reference times the reference CPU solver alone (rank 0), each step a
+bounded sample of the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "EG solve GTEPS (n=2^20, Zipf(2) out-degree, int64 credits)"
+UNIT = "GTEPS"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--workload", choices=["cfg1", "cfg2", "cfg3"], default="cfg2")
+    ap.add_argument("--n", type=int, default=0, help="override the vertex count (smaller cases)")
+    ap.add_argument("--e2e-steps", type=int, default=0, help="e2e steps (default: --steps)")
+    ap.add_argument("--cpu-sample-s", type=float, default=10.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--variant", type=int, default=0)
+    ap.add_argument("--max-rounds", type=int, default=-1,
+                    help="profiling aid: cap every solve at this many rounds (the line is then not a benchmark)")
+    return ap.parse_args()
+
+
+def load_workload(name: str, n: int):
+    from egsolver_b200 import workloads
+
+    fn = getattr(workloads, name)
+    return fn(n) if n else fn()
+
+
+def workload_config(name: str, game) -> dict:
+    deg = np.diff(game.row_ptr)
+    return {"workload": {"cfg1": "random 4-regular game", "cfg2": "single large sparse game",
+                         "cfg3": "dense clique game"}[name],
+            "n": game.num_nodes, "m": game.num_edges, "max_out_degree": int(deg.max()),
+            "mean_out_degree": round(float(deg.mean()), 3), "weights": f"+-{game.max_abs_weight}",
+            "credits": "int64", "seed": "0xE6+cfg", "l2": "flushed (256 MB write) before every step"}
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.lines: list[str] = []
+        self.proc = None
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                                          "-lms", "200", "-i", str(device)], stdout=subprocess.PIPE,
+                                         stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax.append(float(parts[2]))
+            except ValueError:
+                continue
+            for nm, val in zip(names, parts[5:9]):
+                if val.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_peak():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def lift_traffic_bytes(st, credit_bytes: int) -> float:
+    """Algorithmic bytes of one lifting-kernel launch:
+    per scanned edge: successor 4 + weight 4 + successor credit S;
+    per lifted vertex: two row offsets 8 + own credit S;
+    per raised credit: the write S + two CSC offsets 8;
+    per predecessor pushed: its id 4 + its frontier word 4."""
+    S = credit_bytes
+    return (st.edges * (8 + S) + st.lifts * (8 + S) + st.changes * (S + 8) + st.pushes * 8)
+
+
+def cpu_sample(game, seconds: float, kind_pref: str = "reference"):
+    """Times the reference worklist solver on its first P pops of `game`.
+    Returns (gteps, edges, secs, pops, kind)."""
+    from oracle import oracle as O
+
+    use_ref = kind_pref == "reference" and O.ref_available()
+    # calibrate P with the restatement (same pop sequence as the reference)
+    P = 2_000_000
+    _, st = O.eg_solve(game, bits=32, max_loop_=P)
+    t0 = time.perf_counter()
+    _, st = O.eg_solve(game, bits=32, max_loop_=P)
+    dt = time.perf_counter() - t0
+    P = max(P, int(P * seconds / max(dt, 1e-3)))
+    _, st = O.eg_solve(game, bits=32, max_loop_=P)  # edges of exactly these pops (untimed)
+    edges = st["edges"]
+    if use_ref:
+        _, rst = O.ref_cpu_solve(game, "eg", threads=1, max_loop_=P)
+        secs = rst["seconds"]  # the reference's own solving time (cpu_solver(), transpose included)
+    else:
+        t0 = time.perf_counter()
+        O.eg_solve(game, bits=32, max_loop_=P)
+        secs = time.perf_counter() - t0
+    return edges / secs / 1e9, edges, secs, P, "reference" if use_ref else "port"
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    game = load_workload(args.workload, args.n)
+    from oracle import oracle as O
+
+    use_ref = O.ref_available()
+    seconds = max(1.0, args.cpu_sample_s / 2)
+    P = 1_000_000
+    t0 = time.perf_counter()
+    _, st = O.eg_solve(game, bits=32, max_loop_=P)
+    dt = time.perf_counter() - t0
+    P = max(P, int(P * seconds / max(dt, 1e-3)))
+    _, st = O.eg_solve(game, bits=32, max_loop_=P)
+    edges = st["edges"]
+
+    def step():
+        # the reference's own "Solving time" (cpu_solver(), transpose included)
+        if use_ref:
+            _, rst = O.ref_cpu_solve(game, "eg", threads=1, max_loop_=P)
+            return rst["seconds"]
+        t = time.perf_counter()
+        O.eg_solve(game, bits=32, max_loop_=P)
+        return time.perf_counter() - t
+
+    for _ in range(min(args.warmup, 1)):
+        step()
+    times = [step() for _ in range(args.steps)]
+    total = sum(times)
+    value = edges * args.steps / total / 1e9
+    kind = "reference" if use_ref else "port"
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": min(args.warmup, 1), "ms_per_step": 1e3 * total / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int32", "data": "synthetic",
+            "config": workload_config(args.workload, game),
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": 1, "kind": kind,
+                             "sample": f"first {P} worklist pops of EG_cpu_solver (reference --eg {P}) on the "
+                                       f"same game, {edges} edges relaxed per step"},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+        return
+    import torch
+
+    import egsolver_b200 as eg
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    torch.cuda.set_device(local)
+    game = load_workload(args.workload, args.n)
+    credit_bits = 64
+    cfg = workload_config(args.workload, game)
+    cfg["parallelism"] = f"replicas x{world}" if world > 1 else "single GPU"
+
+    res = eg.ResidentGame(game, device=local)
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.int32, device=f"cuda:{local}")
+    kw = dict(credit_bits=credit_bits, device=local, variant=args.variant, max_rounds=args.max_rounds)
+    capped = args.max_rounds >= 0
+    for _ in range(args.warmup):
+        flush.fill_(1)
+        torch.cuda.synchronize()
+        res.solve(raise_on_error=not capped, **kw)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    sampler = ClockSampler(local)
+    stats = []
+    t_wall = time.perf_counter()
+    for _ in range(args.steps):
+        flush.fill_(1)
+        torch.cuda.synchronize()
+        _, st = res.solve(raise_on_error=not capped, **kw)
+        stats.append(st)
+    torch.cuda.synchronize()
+    t_wall = time.perf_counter() - t_wall
+    clocks = sampler.stop()
+    if dist:
+        dist.barrier()
+    dev_ms = sum(s.solve_ms for s in stats)
+    edges = sum(s.edges for s in stats)
+    lift_ms = sum(s.lift_ms for s in stats)
+    launches = sum(s.kernel_launches for s in stats)
+    # correctness guard on the last timed solve: a fixed point of the lifting operator
+    credits = res.credits(64)
+    res.free()
+    if dist:
+        t = torch.tensor([dev_ms], dtype=torch.float64, device=f"cuda:{local}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e = torch.tensor([float(edges)], dtype=torch.float64, device=f"cuda:{local}")
+        dist.all_reduce(e, op=dist.ReduceOp.SUM)
+        dev_ms_max, edges_all = float(t.item()), float(e.item())
+    else:
+        dev_ms_max, edges_all = dev_ms, float(edges)
+    value = edges_all / (dev_ms_max / 1e3) / 1e9
+
+    # e2e through the one-call API with pinned host buffers
+    e2e = None
+    if not args.no_e2e and not capped:
+        pin_rp = torch.from_numpy(game.row_ptr).pin_memory()
+        pin_sc = torch.from_numpy(game.succ).pin_memory()
+        pin_wt = torch.from_numpy(game.weight).pin_memory()
+        pgame = eg.Game(row_ptr=pin_rp.numpy(), succ=pin_sc.numpy(), weight=pin_wt.numpy(),
+                        num_nodes0=game.num_nodes0, max_abs_weight=game.max_abs_weight)
+        assert pgame.row_ptr.ctypes.data == pin_rp.data_ptr()
+        out = torch.empty(game.num_nodes, dtype=torch.int64).pin_memory()
+        import ctypes
+
+        cg = pgame.c_struct()
+        opts = eg.make_opts(**kw)
+        est = eg._ffi.EgStats()
+        k = args.e2e_steps or args.steps
+        e_edges, e_secs = 0, 0.0
+        for i in range(k + 1):
+            flush.fill_(1)
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            s = eg.lib().eg_solve_i64(ctypes.byref(cg), ctypes.byref(opts), out.data_ptr(), ctypes.byref(est))
+            dt = time.perf_counter() - t0
+            if s != 0:
+                raise RuntimeError(eg.lib().eg_last_error().decode())
+            if i > 0:  # first call warms the allocator / module load
+                e_edges += est.edges
+                e_secs += dt
+        if not np.array_equal(out.numpy(), credits):
+            raise RuntimeError("e2e credits differ from the resident solve")
+        h2d = game.row_ptr.nbytes + game.succ.nbytes + game.weight.nbytes
+        e2e = {"value": e_edges / e_secs / 1e9, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
+               "d2h_bytes_per_step": int(game.num_nodes * 8), "steps": k,
+               "ms_per_step": 1e3 * e_secs / k}
+
+    from oracle import oracle as O  # the checker, outside every timed region
+
+    bad = 0 if capped else O.count_inconsistent(game, credits)
+    if bad:
+        raise RuntimeError(f"{bad} vertices are not at a fixed point after the solve")
+
+    last = stats[-1]
+    peak, peak_kind = measured_peak()
+    lift_bytes = lift_traffic_bytes(last, credit_bits // 8)
+    achieved = lift_bytes / (last.lift_ms / 1e3) / 1e9
+    traffic = None
+    tf = ROOT / "profiles" / "lift_traffic.json"
+    if tf.exists():
+        try:
+            d = json.loads(tf.read_text())
+            if d.get("workload") == cfg["workload"] and d.get("n") == game.num_nodes:
+                traffic = d.get("dram_bytes_per_launch")
+        except (ValueError, KeyError):
+            traffic = None
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                "traffic": traffic, "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)",
+                "kernel": "k_lift (persistent lifting kernel)", "algorithmic_bytes_per_launch": lift_bytes}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        g, ed, secs, P, kind = cpu_sample(game, args.cpu_sample_s)
+        cpu = {"value": g, "unit": UNIT, "cores": 1, "kind": kind,
+               "sample": f"first {P} worklist pops of EG_cpu_solver (reference --eg {P}) on the same game: "
+                         f"{ed} edges in {secs:.2f} s"}
+
+    if rank == 0:
+        if capped:
+            cfg["profiling_cap_rounds"] = args.max_rounds
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": dev_ms_max / args.steps, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "int64", "data": "synthetic", "config": cfg,
+                "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(launches),
+                "clocks": clocks,
+                "solve": {"rounds": last.rounds, "lifts": last.lifts, "edges": last.edges, "changes": last.changes,
+                          "pushes": last.pushes, "num_top": last.num_top, "mg": last.mg,
+                          "solve_ms": last.solve_ms, "lift_ms": last.lift_ms, "grid": last.grid,
+                          "block": last.block, "wall_s_timed": t_wall}}
+        print(json.dumps(line), flush=True)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

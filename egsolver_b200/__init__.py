@@ -21,7 +21,8 @@ from . import _ffi
 from ._ffi import (EG_TOP32, EG_TOP64, VARIANT_AUTO, VARIANT_CTA, VARIANT_SMEM, VARIANT_THREAD,  # noqa: F401
                    VARIANT_WARP)
 
-__all__ = ["Game", "EGError", "Stats", "solve", "ResidentGame", "generate", "read_game", "read_game_text",
+__all__ = ["Game", "EGError", "Stats", "solve", "ResidentGame", "Batch", "BatchStats", "threshold_game",
+           "generate", "read_game", "read_game_text",
            "csr2csc", "compute_mg", "default_max_loop", "device_count", "CancelFlag", "EG_TOP32", "EG_TOP64",
            "lib"]
 
@@ -117,6 +118,10 @@ class Stats:
     variant_large: int
     small_max_deg: int
     large_min_deg: int
+    changes: int
+    pushes: int
+    grid: int
+    block: int
 
     @classmethod
     def from_c(cls, s: _ffi.EgStats) -> "Stats":
@@ -241,6 +246,111 @@ class CancelFlag:
         if self.ptr:
             lib().eg_cancel_flag_free(self.ptr)
             self.ptr = None
+
+
+@dataclass
+class BatchStats:
+    num_games: int
+    thresholds: int
+    total_nodes: int
+    total_edges: int
+    rounds_max: int
+    rounds_sum: int
+    lifts: int
+    edges: int
+    num_top: int
+    solve_ms: float
+    block: int
+    grid: int
+    games_failed: int
+    graph_replayed: int
+
+    @property
+    def gteps(self) -> float:
+        return self.edges / (self.solve_ms * 1e6) if self.solve_ms > 0 else 0.0
+
+
+class Batch:
+    """Many games x K mean-payoff thresholds solved in one persistent launch
+    (eg_batch_*).  Threshold p of game g turns every weight w into w*d - p."""
+
+    def __init__(self, games: list[Game], thresholds: int, scale: int = 1, block: int = 0, device: int = 0,
+                 max_rounds: int = -1, timeout_ms: float = 0.0, use_graph: bool = False):
+        self._h = C.c_void_p()
+        self._keep = [g.c_struct() for g in games]
+        arr = (_ffi.EgGame * len(games))(*self._keep)
+        o = _ffi.EgBatchOpts()
+        o.thresholds = thresholds
+        o.scale = scale
+        o.block = block
+        o.device = device
+        o.max_rounds = max_rounds
+        o.timeout_ms = timeout_ms
+        o.use_graph = 1 if use_graph else 0
+        _check(lib().eg_batch_create(arr, len(games), C.byref(o), C.byref(self._h)))
+        self.sizes = [g.num_nodes for g in games]
+        self.K = thresholds
+
+    def set_thresholds(self, p) -> None:
+        a = np.ascontiguousarray(p, dtype=np.int32).reshape(-1)
+        if a.size != len(self.sizes) * self.K:
+            raise ValueError("need num_games * K thresholds")
+        _check(lib().eg_batch_set_thresholds(self._h, a.ctypes.data))
+
+    def solve(self, raise_on_error: bool = True) -> tuple[int, BatchStats]:
+        st = _ffi.EgBatchStats()
+        status = lib().eg_batch_solve(self._h, C.byref(st))
+        if raise_on_error:
+            _check(status)
+        return status, BatchStats(**st.as_dict())
+
+    def credits(self, game: int) -> np.ndarray:
+        """Credits of one game as a (K, n) int64 array (TOP = EG_TOP64)."""
+        n = self.sizes[game]
+        out = np.zeros(self.K * n, dtype=np.int64)
+        _check(lib().eg_batch_credits(self._h, game, out.ctypes.data))
+        return out.reshape(self.K, n)
+
+    def game_result(self, game: int) -> tuple[int, int]:
+        r = C.c_int64()
+        s = C.c_int32()
+        _check(lib().eg_batch_game_result(self._h, game, C.byref(r), C.byref(s)))
+        return int(r.value), int(s.value)
+
+    def tune(self) -> int:
+        b = C.c_int32()
+        _check(lib().eg_batch_tune(self._h, C.byref(b)))
+        return int(b.value)
+
+    @property
+    def device_bytes(self) -> int:
+        return int(lib().eg_batch_device_bytes(self._h))
+
+    def free(self) -> None:
+        if self._h:
+            lib().eg_batch_free(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.free()
+
+
+def threshold_game(game: Game, p: int, d: int) -> Game:
+    """The energy game of the mean-payoff query (weights w*d - p), for checking."""
+    w = game.weight.astype(np.int64) * d - p
+    if w.min() < -2**31 or w.max() >= 2**31:
+        raise OverflowError("shifted weights do not fit int32")
+    return Game(row_ptr=game.row_ptr, succ=game.succ, weight=w.astype(np.int32), num_nodes0=game.num_nodes0,
+                owner=game.owner, ext_id=game.ext_id)
 
 
 def _own_to_game(og_ptr) -> Game:

@@ -67,7 +67,11 @@ class EgStats(C.Structure):
         ("variant_large", C.c_int32),
         ("small_max_deg", C.c_int32),
         ("large_min_deg", C.c_int32),
-        ("reserved", C.c_int32 * 4),
+        ("changes", C.c_int64),
+        ("pushes", C.c_int64),
+        ("grid", C.c_int32),
+        ("block", C.c_int32),
+        ("reserved", C.c_int32 * 2),
     ]
 
     def as_dict(self) -> dict:
@@ -92,6 +96,42 @@ class EgReadOpts(C.Structure):
         ("rnd_hi", C.c_int32),
         ("rnd_seed", C.c_uint64),
     ]
+
+
+class EgBatchOpts(C.Structure):
+    _fields_ = [
+        ("thresholds", C.c_int32),
+        ("scale", C.c_int32),
+        ("block", C.c_int32),
+        ("device", C.c_int32),
+        ("max_rounds", C.c_int64),
+        ("timeout_ms", C.c_double),
+        ("use_graph", C.c_int32),
+        ("reserved", C.c_int32 * 7),
+    ]
+
+
+class EgBatchStats(C.Structure):
+    _fields_ = [
+        ("num_games", C.c_int32),
+        ("thresholds", C.c_int32),
+        ("total_nodes", C.c_int64),
+        ("total_edges", C.c_int64),
+        ("rounds_max", C.c_int64),
+        ("rounds_sum", C.c_int64),
+        ("lifts", C.c_int64),
+        ("edges", C.c_int64),
+        ("num_top", C.c_int64),
+        ("solve_ms", C.c_double),
+        ("block", C.c_int32),
+        ("grid", C.c_int32),
+        ("games_failed", C.c_int32),
+        ("graph_replayed", C.c_int32),
+        ("reserved", C.c_int32 * 4),
+    ]
+
+    def as_dict(self) -> dict:
+        return {k: getattr(self, k) for k, _ in self._fields_ if k != "reserved"}
 
 
 # every symbol the header declares, with (restype, argtypes)
@@ -124,6 +164,14 @@ SIGNATURES = {
     "eg_parse_text": (_I32, [C.c_char_p, C.c_size_t, _P]),
     "eg_read_file_bytes": (_I32, [C.c_char_p, C.POINTER(C.c_void_p), C.POINTER(C.c_size_t)]),
     "eg_generate": (_I32, [_I32, _I32, _I32, _I32, _I32, C.c_uint64, C.POINTER(C.POINTER(EgOwnedGame))]),
+    "eg_batch_create": (_I32, [C.POINTER(EgGame), _I32, C.POINTER(EgBatchOpts), C.POINTER(_P)]),
+    "eg_batch_set_thresholds": (_I32, [_P, _P]),
+    "eg_batch_solve": (_I32, [_P, C.POINTER(EgBatchStats)]),
+    "eg_batch_credits": (_I32, [_P, _I32, _P]),
+    "eg_batch_game_result": (_I32, [_P, _I32, C.POINTER(_I64), C.POINTER(_I32)]),
+    "eg_batch_tune": (_I32, [_P, C.POINTER(_I32)]),
+    "eg_batch_device_bytes": (_I64, [_P]),
+    "eg_batch_free": (None, [_P]),
 }
 
 _lib = None

@@ -38,6 +38,10 @@ namespace {
 
 constexpr unsigned long long kWaitLimitNs = 5ull * 1000ull * 1000ull * 1000ull; /* 5 s per barrier wait */
 constexpr int kPrepBlock = 256;
+/* AUTO lifts a game with one CTA (frontier in shared memory) up to this
+ * many edges; larger games use the persistent grid. */
+constexpr long long kSmallGameEdges = 1 << 17;
+constexpr int kSmallGameMaxPad = 1 << 19;
 
 inline unsigned grid_for(long long items, int block, int cap = 148 * 32)
 {
@@ -149,8 +153,6 @@ static eg_status check_lanes(const eg_opts *o)
         if (k != 1 && k != 2 && k != 4 && k != 8 && k != 16 && k != 32)
             return eg_set_error(EG_ERR_INVALID, "lanes_per_vertex must be 1, 2, 4, 8, 16 or 32 (got %d)", k);
     }
-    if (o && o->variant == EG_VARIANT_SMEM)
-        return eg_set_error(EG_ERR_INVALID, "EG_VARIANT_SMEM is a batch-solver variant");
     if (o && (o->variant < 0 || o->variant > EG_VARIANT_SMEM))
         return eg_set_error(EG_ERR_INVALID, "unknown variant %d", o->variant);
     if (o && o->credit_bits != 0 && o->credit_bits != 32 && o->credit_bits != 64)
@@ -431,8 +433,16 @@ extern "C" eg_status eg_dgame_solve(eg_dgame *g, const eg_opts *opts_in, eg_stat
     }
     p.nclasses = nc;
     int grid = 0, block = 0;
+    const bool small = n_pad <= kSmallGameMaxPad &&
+                       (opts->variant == EG_VARIANT_SMEM || (opts->variant == EG_VARIANT_AUTO && g->m <= kSmallGameEdges));
     EG_CUDA(cudaEventRecord(g->ev[1], st));
-    EG_TRY(launch_lift(p, bits, st, &grid, &block));
+    if (small) {
+        EG_TRY(launch_lift_cta(p, bits, st));
+        grid = 1;
+        block = 1024;
+    } else {
+        EG_TRY(launch_lift(p, bits, st, &grid, &block));
+    }
     g->launches++;
     EG_CUDA(cudaEventRecord(g->ev[2], st));
     launch_count_top(bits, n_pad, g->d_F, &g->d_ctrl->num_top, st);
@@ -462,6 +472,10 @@ extern "C" eg_status eg_dgame_solve(eg_dgame *g, const eg_opts *opts_in, eg_stat
         stats->variant_small = g->groups[0];
         stats->variant_mid = g->bb.nb > 2 ? g->groups[1] : g->groups[0];
         stats->variant_large = g->groups[g->bb.nb - 1];
+        stats->changes = (int64_t)ctrl.changes;
+        stats->pushes = (int64_t)ctrl.pushes;
+        stats->grid = grid;
+        stats->block = block;
     }
     if (ctrl.stop == EG_ERR_LOOPCAP)
         return eg_set_error(EG_ERR_LOOPCAP, "round cap %lld reached with work left", (long long)opts->max_rounds);

@@ -1,0 +1,698 @@
+/*
+ * eg_batch.cu -- batched solving of many games at K mean-payoff thresholds
+ * in one persistent launch.
+ *
+ * Layout: the games are packed into one device-resident multi-CSR (global
+ * vertex ids, no edge crosses games), with one CSC built by the same stable
+ * counting sort as the single-game path.  Credits are stored vertex-major
+ * with the K thresholds contiguous, f[(v * K) + k], so the K lanes that
+ * lift vertex v for the K thresholds read one successor's K credits as a
+ * single contiguous row.
+ *
+ * Kernel: every CTA takes a game from a device queue (largest games first),
+ * computes MG_k = sum_v max(0, p_k - d * min_w(v)) and the initial frontier
+ * for all thresholds, then runs the lifting rounds of that game alone with
+ * CTA barriers; its frontier bitmaps live in shared memory, so the push of
+ * a predecessor is a shared-memory atomicOr.  The lift of vertex v for
+ * threshold k is the reference's (reference src/dev_EG_alg.cu:84-109) on the
+ * weights w * d - p_k.  No wait in this kernel spins: rounds end at
+ * __syncthreads and games come from an atomic counter.
+ */
+#include "eg_prep.cuh"
+
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <numeric>
+#include <vector>
+
+using namespace eg;
+
+#define EG_CUDA(call)                                                                                  \
+    do {                                                                                               \
+        cudaError_t _e = (call);                                                                       \
+        if (_e != cudaSuccess)                                                                         \
+            return eg_set_error(_e == cudaErrorMemoryAllocation ? EG_ERR_OOM : EG_ERR_CUDA,             \
+                                "%s failed: %s (%s:%d)", #call, cudaGetErrorString(_e), __FILE__, __LINE__); \
+    } while (0)
+
+#define EG_TRY(call)                                                                                   \
+    do {                                                                                               \
+        eg_status _s = (call);                                                                         \
+        if (_s != EG_OK) return _s;                                                                    \
+    } while (0)
+
+namespace {
+
+constexpr int kMaxGameNodes = 1 << 19;
+
+struct BatchCtrl {
+    int next_game;
+    int pad;
+    unsigned long long lifts, edges, num_top;
+    unsigned long long t_start;
+};
+
+struct BatchParams {
+    const long long *node_off;   /* num_games + 1                       */
+    const int *order;            /* game queue order (largest first)    */
+    const int *P;                /* global edge offsets, total_nodes+1  */
+    const int2 *E;               /* {global successor, weight}          */
+    const int *CP;               /* CSC offsets                         */
+    const int *CS;               /* CSC predecessors (global ids)       */
+    const unsigned char *owner;
+    const int *minw, *maxw;      /* per vertex                          */
+    const int *thr;              /* p[g * K + k]                        */
+    long long *F;                /* credits [v * K + k]                 */
+    long long *rounds;           /* per game                            */
+    int *status;                 /* per game                            */
+    BatchCtrl *ctrl;
+    int num_games, K, d;
+    int words_max;               /* shared bitmap words per buffer      */
+    long long max_rounds;
+    unsigned long long timeout_ns;
+};
+
+__device__ __forceinline__ int nth_bit(uint32_t w, int k)
+{
+    int pos = 0;
+#pragma unroll
+    for (int s = 16; s > 0; s >>= 1) {
+        const uint32_t low = w & ((1u << s) - 1u);
+        const int c = __popc(low);
+        if (k >= c) {
+            k -= c;
+            w >>= s;
+            pos += s;
+        } else {
+            w = low;
+        }
+    }
+    return pos;
+}
+
+__device__ __forceinline__ long long ominus64(long long a, long long b, long long mg)
+{
+    const long long t = (long long)INT64_MAX;
+    const long long x = a - b;
+    return (a < t && x <= mg) ? (x > 0 ? x : 0) : t;
+}
+
+/* KP lanes per vertex (KP >= K, a power of two); lane k serves threshold k. */
+template <int KP>
+__global__ void __launch_bounds__(1024) k_batch_solve(const __grid_constant__ BatchParams p)
+{
+    extern __shared__ uint32_t sm[];
+    __shared__ int s_game;
+    __shared__ int s_ctr[2];
+    __shared__ long long s_mg[KP];
+    __shared__ int s_p[KP];
+    constexpr int NG = 32 / KP;
+    const int tid = threadIdx.x, lane = tid & 31;
+    const int grp = lane / KP, gl = lane % KP;
+    const unsigned gmask = (KP == 32) ? 0xffffffffu : (((1u << KP) - 1u) << (grp * KP));
+    const int K = p.K;
+    const long long d = p.d;
+    const long long TOP = (long long)INT64_MAX;
+    unsigned long long lifts = 0, edges = 0, ntop = 0;
+    if (blockIdx.x == 0 && tid == 0) p.ctrl->t_start = globaltimer_ns();
+    for (;;) {
+        if (tid == 0) s_game = atomicAdd(&p.ctrl->next_game, 1);
+        __syncthreads();
+        const int gi = s_game;
+        if (gi >= p.num_games) break;
+        const int g = p.order[gi];
+        const long long base = p.node_off[g];
+        const int n = (int)(p.node_off[g + 1] - base);
+        const int W = (n + 31) >> 5;
+        uint32_t *cur = sm, *nxt = sm + p.words_max;
+        if (tid < KP) {
+            s_p[tid] = p.thr[(long long)g * K + (tid < K ? tid : 0)];
+            s_mg[tid] = 0;
+        }
+        if (tid < 2) s_ctr[tid] = 0;
+        for (int w = tid; w < W; w += blockDim.x) {
+            cur[w] = 0;
+            nxt[w] = 0;
+        }
+        __syncthreads();
+        /* f = 0, MG per threshold, initial frontier (any threshold) */
+        for (int v = tid; v < n; v += blockDim.x) {
+            const long long gv = base + v;
+            for (int k = 0; k < K; k++) p.F[gv * K + k] = 0;
+            const long long lo = (long long)p.minw[gv] * d, hi = (long long)p.maxw[gv] * d;
+            const int own = p.owner[gv];
+            bool act = false;
+            for (int k = 0; k < K; k++) act |= own ? (lo - s_p[k] < 0) : (hi - s_p[k] < 0);
+            if (act) atomicOr(&cur[v >> 5], 1u << (v & 31));
+        }
+        for (int k = 0; k < K; k++) {
+            long long s = 0;
+            for (int v = tid; v < n; v += blockDim.x) {
+                const long long x = (long long)s_p[k] - (long long)p.minw[base + v] * d;
+                s += x > 0 ? x : 0;
+            }
+#pragma unroll
+            for (int off = 16; off > 0; off >>= 1) s += __shfl_xor_sync(0xffffffffu, s, off);
+            if (lane == 0 && s) atomicAdd((unsigned long long *)&s_mg[k], (unsigned long long)s);
+        }
+        __syncthreads();
+        const long long pk = s_p[gl];
+        const long long mgk = s_mg[gl];
+        const bool valid = gl < K;
+        long long r = 0;
+        int st = EG_OK;
+        for (;;) {
+            if (tid == 0) s_ctr[(r + 1) & 1] = 0;
+            int any_new = 0;
+            for (;;) {
+                int w0 = 0;
+                if (lane == 0) w0 = atomicAdd(&s_ctr[r & 1], 1);
+                w0 = __shfl_sync(0xffffffffu, w0, 0);
+                if (w0 >= W) break;
+                uint32_t word = cur[w0];
+                __syncwarp();
+                if (lane == 0 && word) cur[w0] = 0;
+                while (word) {
+                    const int c = __popc(word);
+                    if (grp < c) {
+                        const int v = (w0 << 5) + nth_bit(word, grp);
+                        const long long gv = base + v;
+                        const int own = p.owner[gv];
+                        long long acc = own ? 0 : TOP;
+                        const int eb = p.P[gv], ee = p.P[gv + 1];
+                        for (int e = eb; e < ee; e++) {
+                            const int2 q = __ldg(p.E + e);
+                            if (valid) {
+                                const long long val = ominus64(p.F[(long long)q.x * K + gl], (long long)q.y * d - pk, mgk);
+                                acc = own ? (val > acc ? val : acc) : (val < acc ? val : acc);
+                            }
+                        }
+                        bool ch = false;
+                        if (valid) {
+                            const long long old = p.F[gv * K + gl];
+                            if (old < acc) {
+                                p.F[gv * K + gl] = acc;
+                                ch = true;
+                            }
+                        }
+                        const unsigned chm = __ballot_sync(gmask, ch) & gmask;
+                        if (chm) {
+                            const int cb = p.CP[gv], ce = p.CP[gv + 1];
+                            for (int j = cb + gl; j < ce; j += KP) {
+                                const int pr = (int)(p.CS[j] - base);
+                                const uint32_t bit = 1u << (pr & 31);
+                                if (!(atomicOr(&nxt[pr >> 5], bit) & bit)) any_new = 1;
+                            }
+                        }
+                        if (gl == 0) {
+                            lifts++;
+                            edges += (unsigned long long)(ee - eb) * (unsigned long long)K;
+                        }
+                    }
+                    if (c <= NG) {
+                        word = 0;
+                    } else {
+                        const int last = nth_bit(word, NG - 1);
+                        word &= ~((2u << last) - 1u);
+                    }
+                }
+            }
+            r++;
+            const int cont = __syncthreads_or(any_new);
+            if (!cont) break;
+            if (p.max_rounds >= 0 && r >= p.max_rounds) {
+                st = EG_ERR_LOOPCAP;
+                break;
+            }
+            const int late = __syncthreads_or(tid == 0 && p.timeout_ns &&
+                                              globaltimer_ns() - p.ctrl->t_start > p.timeout_ns);
+            if (late) {
+                st = EG_ERR_TIMEOUT;
+                break;
+            }
+            uint32_t *t = cur;
+            cur = nxt;
+            nxt = t;
+        }
+        /* TOP count of this game (all thresholds) */
+        for (long long i = tid; i < (long long)n * K; i += blockDim.x) ntop += (p.F[base * K + i] == TOP);
+        if (tid == 0) {
+            p.rounds[g] = r;
+            p.status[g] = st;
+        }
+        __syncthreads();
+    }
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) {
+        lifts += __shfl_xor_sync(0xffffffffu, lifts, off);
+        edges += __shfl_xor_sync(0xffffffffu, edges, off);
+        ntop += __shfl_xor_sync(0xffffffffu, ntop, off);
+    }
+    if (lane == 0) {
+        atomicAdd(&p.ctrl->lifts, lifts);
+        atomicAdd(&p.ctrl->edges, edges);
+        atomicAdd(&p.ctrl->num_top, ntop);
+    }
+}
+
+/* one warp per vertex of the packed graph: CSC sort input and in-degrees */
+__global__ void k_batch_expand(long long total_nodes, const int *P, const int2 *E, int *key, int *val, int *indeg)
+{
+    const int lane = threadIdx.x & 31;
+    const long long w0 = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const long long nw = ((long long)gridDim.x * blockDim.x) >> 5;
+    for (long long v = w0; v < total_nodes; v += nw) {
+        for (int e = P[v] + lane; e < P[v + 1]; e += 32) {
+            const int s = E[e].x;
+            key[e] = s;
+            val[e] = (int)v;
+            atomicAdd(&indeg[s], 1);
+        }
+    }
+}
+
+typedef void (*batch_kernel_t)(BatchParams);
+
+batch_kernel_t kernel_for(int kp)
+{
+    switch (kp) {
+    case 1: return k_batch_solve<1>;
+    case 2: return k_batch_solve<2>;
+    case 4: return k_batch_solve<4>;
+    case 8: return k_batch_solve<8>;
+    case 16: return k_batch_solve<16>;
+    default: return k_batch_solve<32>;
+    }
+}
+
+int pow2_at_least(int k)
+{
+    int x = 1;
+    while (x < k) x <<= 1;
+    return x;
+}
+
+}  // namespace
+
+struct eg_batch {
+    int device;
+    cudaStream_t st;
+    cudaEvent_t ev0, ev1;
+    int num_games, K, KP, d;
+    long long total_nodes, total_edges;
+    int words_max;
+    int block;
+    long long max_rounds;
+    double timeout_ms;
+    std::vector<long long> node_off_h;
+    long long *node_off;
+    int *order, *P, *CP, *CS, *minw, *maxw, *thr, *status;
+    int2 *E;
+    unsigned char *owner;
+    long long *F, *rounds;
+    BatchCtrl *ctrl;
+    size_t bytes;
+    bool thresholds_set, solved;
+    bool use_graph;
+    cudaGraph_t graph;
+    cudaGraphExec_t graph_exec;
+    int graph_block;
+};
+
+template <class T>
+static eg_status balloc(eg_batch *b, T **p, size_t count)
+{
+    const size_t bytes = std::max<size_t>(count * sizeof(T), 16);
+    cudaError_t e = cudaMalloc((void **)p, bytes);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        *p = nullptr;
+        return eg_set_error(EG_ERR_OOM, "cudaMalloc of %zu bytes failed: %s", bytes, cudaGetErrorString(e));
+    }
+    b->bytes += bytes;
+    return EG_OK;
+}
+
+extern "C" void eg_batch_free(eg_batch *b)
+{
+    if (!b) return;
+    cudaSetDevice(b->device);
+    if (b->st) cudaStreamSynchronize(b->st);
+    if (b->graph_exec) cudaGraphExecDestroy(b->graph_exec);
+    if (b->graph) cudaGraphDestroy(b->graph);
+    void *ptrs[] = {b->node_off, b->order, b->P, b->CP, b->CS, b->minw, b->maxw, b->thr,
+                    b->status, b->E, b->owner, b->F, b->rounds, b->ctrl};
+    for (void *q : ptrs)
+        if (q) cudaFree(q);
+    if (b->ev0) cudaEventDestroy(b->ev0);
+    if (b->ev1) cudaEventDestroy(b->ev1);
+    if (b->st) cudaStreamDestroy(b->st);
+    delete b;
+}
+
+extern "C" int64_t eg_batch_device_bytes(const eg_batch *b) { return b ? (int64_t)b->bytes : 0; }
+
+extern "C" eg_status eg_batch_create(const eg_game *games, int32_t num_games, const eg_batch_opts *opts, eg_batch **out)
+{
+    if (!games || num_games <= 0 || !opts || !out) return eg_set_error(EG_ERR_INVALID, "bad batch arguments");
+    if (opts->thresholds < 1 || opts->thresholds > EG_BATCH_MAX_K)
+        return eg_set_error(EG_ERR_INVALID, "thresholds must be in [1, %d]", EG_BATCH_MAX_K);
+    if (opts->scale < 1) return eg_set_error(EG_ERR_INVALID, "scale d must be >= 1");
+    if (opts->block && (opts->block < 64 || opts->block > 1024 || (opts->block & 31)))
+        return eg_set_error(EG_ERR_INVALID, "block must be a multiple of 32 in [64, 1024]");
+    long long tn = 0, tm = 0;
+    int nmax = 0;
+    for (int g = 0; g < num_games; g++) {
+        eg_status s = eg_validate(&games[g]);
+        if (s != EG_OK) return eg_set_error(s, "game %d: %s", g, eg_last_error());
+        if (games[g].num_nodes > kMaxGameNodes)
+            return eg_set_error(EG_ERR_INVALID, "game %d has %d vertices; the batch path holds at most %d per game",
+                                g, games[g].num_nodes, kMaxGameNodes);
+        tn += games[g].num_nodes;
+        tm += games[g].num_edges;
+        nmax = std::max(nmax, games[g].num_nodes);
+    }
+    if (tn >= (long long)INT32_MAX - 64 || tm >= (long long)INT32_MAX - 64)
+        return eg_set_error(EG_ERR_INVALID, "batch too large (%lld vertices, %lld edges)", tn, tm);
+    int count = 0;
+    if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0) {
+        cudaGetLastError();
+        return eg_set_error(EG_ERR_NO_DEVICE, "no CUDA device available");
+    }
+    EG_CUDA(cudaSetDevice(opts->device));
+    eg_batch *b = new eg_batch();
+    b->device = opts->device;
+    b->num_games = num_games;
+    b->K = opts->thresholds;
+    b->KP = pow2_at_least(opts->thresholds);
+    b->d = opts->scale;
+    b->total_nodes = tn;
+    b->total_edges = tm;
+    b->words_max = (nmax + 31) / 32;
+    b->block = opts->block ? opts->block : 256;
+    b->max_rounds = opts->max_rounds;
+    b->timeout_ms = opts->timeout_ms;
+    b->use_graph = opts->use_graph != 0;
+    /* host packing: global ids, owners, min/max out-weight */
+    std::vector<int> P((size_t)tn + 1), minw((size_t)tn), maxw((size_t)tn);
+    std::vector<int2> E((size_t)tm);
+    std::vector<unsigned char> own((size_t)tn);
+    b->node_off_h.assign((size_t)num_games + 1, 0);
+    long long vb = 0, eb = 0;
+    for (int g = 0; g < num_games; g++) {
+        const eg_game &G = games[g];
+        b->node_off_h[g] = vb;
+        for (int v = 0; v < G.num_nodes; v++) {
+            P[(size_t)(vb + v)] = (int)(eb + G.row_ptr[v]);
+            own[(size_t)(vb + v)] = G.owner ? G.owner[v] : (unsigned char)(v >= G.num_nodes0);
+            int mn = INT32_MAX, mx = INT32_MIN;
+            for (long long j = G.row_ptr[v]; j < G.row_ptr[v + 1]; j++) {
+                const int w = G.weight[j];
+                E[(size_t)(eb + j)] = make_int2((int)(vb + G.succ[j]), w);
+                mn = std::min(mn, w);
+                mx = std::max(mx, w);
+            }
+            minw[(size_t)(vb + v)] = mn;
+            maxw[(size_t)(vb + v)] = mx;
+        }
+        vb += G.num_nodes;
+        eb += G.num_edges;
+    }
+    b->node_off_h[num_games] = vb;
+    P[(size_t)tn] = (int)tm;
+    std::vector<int> order((size_t)num_games);
+    std::iota(order.begin(), order.end(), 0);
+    std::stable_sort(order.begin(), order.end(), [&](int a, int c) { return games[a].num_edges > games[c].num_edges; });
+
+    eg_status s = EG_OK;
+    cudaError_t e = cudaStreamCreateWithFlags(&b->st, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaEventCreate(&b->ev0);
+    if (e == cudaSuccess) e = cudaEventCreate(&b->ev1);
+    if (e != cudaSuccess) s = eg_set_error(EG_ERR_CUDA, "stream/event creation failed: %s", cudaGetErrorString(e));
+    if (s == EG_OK) s = balloc(b, &b->node_off, (size_t)num_games + 1);
+    if (s == EG_OK) s = balloc(b, &b->order, (size_t)num_games);
+    if (s == EG_OK) s = balloc(b, &b->P, (size_t)tn + 1);
+    if (s == EG_OK) s = balloc(b, &b->CP, (size_t)tn + 1);
+    if (s == EG_OK) s = balloc(b, &b->CS, (size_t)tm);
+    if (s == EG_OK) s = balloc(b, &b->E, (size_t)tm);
+    if (s == EG_OK) s = balloc(b, &b->owner, (size_t)tn);
+    if (s == EG_OK) s = balloc(b, &b->minw, (size_t)tn);
+    if (s == EG_OK) s = balloc(b, &b->maxw, (size_t)tn);
+    if (s == EG_OK) s = balloc(b, &b->thr, (size_t)num_games * b->K);
+    if (s == EG_OK) s = balloc(b, &b->F, (size_t)tn * b->K);
+    if (s == EG_OK) s = balloc(b, &b->rounds, (size_t)num_games);
+    if (s == EG_OK) s = balloc(b, &b->status, (size_t)num_games);
+    if (s == EG_OK) s = balloc(b, &b->ctrl, 1);
+    if (s != EG_OK) {
+        eg_batch_free(b);
+        return s;
+    }
+    cudaStream_t st = b->st;
+    e = cudaMemcpyAsync(b->node_off, b->node_off_h.data(), sizeof(long long) * ((size_t)num_games + 1),
+                        cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(b->order, order.data(), sizeof(int) * (size_t)num_games, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(b->P, P.data(), sizeof(int) * ((size_t)tn + 1), cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(b->E, E.data(), sizeof(int2) * (size_t)tm, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(b->owner, own.data(), (size_t)tn, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(b->minw, minw.data(), sizeof(int) * (size_t)tn, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(b->maxw, maxw.data(), sizeof(int) * (size_t)tn, cudaMemcpyHostToDevice, st);
+    /* CSC by the stable counting sort, with temporary sort buffers */
+    int *k0 = nullptr, *v0 = nullptr, *k1 = nullptr, *v1 = nullptr, *scr = nullptr;
+    const long long scr_ints = radix_scratch_ints(tm) + scan_scratch_ints(tn + 1) + 64;
+    if (e == cudaSuccess) e = cudaMalloc(&k0, sizeof(int) * (size_t)std::max<long long>(tm, 1));
+    if (e == cudaSuccess) e = cudaMalloc(&v0, sizeof(int) * (size_t)std::max<long long>(tm, 1));
+    if (e == cudaSuccess) e = cudaMalloc(&k1, sizeof(int) * (size_t)std::max<long long>(tm, 1));
+    if (e == cudaSuccess) e = cudaMalloc(&v1, sizeof(int) * (size_t)std::max<long long>(tm, 1));
+    if (e == cudaSuccess) e = cudaMalloc(&scr, sizeof(int) * (size_t)scr_ints);
+    if (e == cudaSuccess) e = cudaMemsetAsync(b->CP, 0, sizeof(int) * ((size_t)tn + 1), st);
+    if (e == cudaSuccess) {
+        long long gr = (tn * 32 + 255) / 256;
+        if (gr > 148 * 32) gr = 148 * 32;
+        k_batch_expand<<<(unsigned)gr, 256, 0, st>>>(tn, b->P, b->E, k0, v0, b->CP);
+        excl_scan(b->CP, tn + 1, scr, st);
+        int *sk, *sv;
+        radix_sort_pairs(k0, v0, k1, v1, tm, bits_for(tn), scr, st, &sk, &sv);
+        e = cudaMemcpyAsync(b->CS, sv, sizeof(int) * (size_t)tm, cudaMemcpyDeviceToDevice, st);
+    }
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    cudaFree(k0);
+    cudaFree(v0);
+    cudaFree(k1);
+    cudaFree(v1);
+    cudaFree(scr);
+    if (e != cudaSuccess) {
+        s = eg_set_error(e == cudaErrorMemoryAllocation ? EG_ERR_OOM : EG_ERR_CUDA, "batch upload failed: %s",
+                         cudaGetErrorString(e));
+        cudaGetLastError();
+        eg_batch_free(b);
+        return s;
+    }
+    *out = b;
+    return EG_OK;
+}
+
+extern "C" eg_status eg_batch_set_thresholds(eg_batch *b, const int32_t *p)
+{
+    if (!b || !p) return eg_set_error(EG_ERR_INVALID, "NULL argument");
+    EG_CUDA(cudaSetDevice(b->device));
+    EG_CUDA(cudaMemcpyAsync(b->thr, p, sizeof(int) * (size_t)b->num_games * b->K, cudaMemcpyHostToDevice, b->st));
+    EG_CUDA(cudaStreamSynchronize(b->st));
+    b->thresholds_set = true;
+    return EG_OK;
+}
+
+static eg_status batch_params(eg_batch *b, BatchParams *p)
+{
+    memset(p, 0, sizeof *p);
+    p->node_off = b->node_off;
+    p->order = b->order;
+    p->P = b->P;
+    p->E = b->E;
+    p->CP = b->CP;
+    p->CS = b->CS;
+    p->owner = b->owner;
+    p->minw = b->minw;
+    p->maxw = b->maxw;
+    p->thr = b->thr;
+    p->F = b->F;
+    p->rounds = b->rounds;
+    p->status = b->status;
+    p->ctrl = b->ctrl;
+    p->num_games = b->num_games;
+    p->K = b->K;
+    p->d = b->d;
+    p->words_max = b->words_max;
+    p->max_rounds = b->max_rounds;
+    p->timeout_ns = b->timeout_ms > 0 ? (unsigned long long)(b->timeout_ms * 1e6) : 0ull;
+    return EG_OK;
+}
+
+/* Enqueues one solve (control reset + persistent kernel) on the stream. */
+static eg_status batch_enqueue(eg_batch *b, int block, int *grid_out)
+{
+    BatchParams p;
+    batch_params(b, &p);
+    batch_kernel_t fn = kernel_for(b->KP);
+    const size_t smem = sizeof(uint32_t) * 2 * (size_t)b->words_max;
+    cudaError_t e = cudaFuncSetAttribute((const void *)fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return eg_set_error(EG_ERR_CUDA, "shared memory request failed: %s", cudaGetErrorString(e));
+    int per_sm = 0;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void *)fn, block, smem);
+    if (e != cudaSuccess || per_sm < 1)
+        return eg_set_error(EG_ERR_CUDA, "batch kernel does not fit (block %d, %zu B shared)", block, smem);
+    int sms = 0;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, b->device);
+    int grid = sms * per_sm;
+    if (grid > b->num_games) grid = b->num_games;
+    EG_CUDA(cudaMemsetAsync(b->ctrl, 0, sizeof(BatchCtrl), b->st));
+    void *args[] = {(void *)&p};
+    EG_CUDA(cudaLaunchKernel((const void *)fn, dim3(grid), dim3(block), args, smem, b->st));
+    *grid_out = grid;
+    return EG_OK;
+}
+
+extern "C" eg_status eg_batch_solve(eg_batch *b, eg_batch_stats *stats)
+{
+    if (!b) return eg_set_error(EG_ERR_INVALID, "batch is NULL");
+    if (!b->thresholds_set) return eg_set_error(EG_ERR_INVALID, "thresholds not set");
+    EG_CUDA(cudaSetDevice(b->device));
+    int grid = 0;
+    bool replay = false;
+    EG_CUDA(cudaEventRecord(b->ev0, b->st));
+    if (b->use_graph) {
+        if (!b->graph_exec || b->graph_block != b->block) {
+            if (b->graph_exec) cudaGraphExecDestroy(b->graph_exec);
+            if (b->graph) cudaGraphDestroy(b->graph);
+            b->graph_exec = nullptr;
+            b->graph = nullptr;
+            /* capture on a side stream so that the timing events stay outside the graph */
+            cudaStream_t cs;
+            EG_CUDA(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
+            EG_CUDA(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
+            cudaStream_t keep = b->st;
+            b->st = cs;
+            eg_status s = batch_enqueue(b, b->block, &grid);
+            b->st = keep;
+            cudaGraph_t gph = nullptr;
+            cudaError_t e = cudaStreamEndCapture(cs, &gph);
+            cudaStreamDestroy(cs);
+            if (s != EG_OK) {
+                if (gph) cudaGraphDestroy(gph);
+                return s;
+            }
+            if (e != cudaSuccess) return eg_set_error(EG_ERR_CUDA, "graph capture failed: %s", cudaGetErrorString(e));
+            b->graph = gph;
+            EG_CUDA(cudaGraphInstantiate(&b->graph_exec, b->graph, 0));
+            b->graph_block = b->block;
+        } else {
+            replay = true;
+        }
+        EG_CUDA(cudaGraphLaunch(b->graph_exec, b->st));
+    } else {
+        EG_TRY(batch_enqueue(b, b->block, &grid));
+    }
+    EG_CUDA(cudaEventRecord(b->ev1, b->st));
+    BatchCtrl c;
+    EG_CUDA(cudaMemcpyAsync(&c, b->ctrl, sizeof c, cudaMemcpyDeviceToHost, b->st));
+    std::vector<long long> rounds((size_t)b->num_games);
+    std::vector<int> status((size_t)b->num_games);
+    EG_CUDA(cudaMemcpyAsync(rounds.data(), b->rounds, sizeof(long long) * rounds.size(), cudaMemcpyDeviceToHost, b->st));
+    EG_CUDA(cudaMemcpyAsync(status.data(), b->status, sizeof(int) * status.size(), cudaMemcpyDeviceToHost, b->st));
+    EG_CUDA(cudaStreamSynchronize(b->st));
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, b->ev0, b->ev1);
+    b->solved = true;
+    int failed = 0;
+    long long rmax = 0, rsum = 0;
+    eg_status first = EG_OK;
+    for (int g = 0; g < b->num_games; g++) {
+        rmax = std::max(rmax, rounds[g]);
+        rsum += rounds[g];
+        if (status[g] != EG_OK) {
+            failed++;
+            if (first == EG_OK) first = (eg_status)status[g];
+        }
+    }
+    if (stats) {
+        memset(stats, 0, sizeof *stats);
+        stats->num_games = b->num_games;
+        stats->thresholds = b->K;
+        stats->total_nodes = b->total_nodes;
+        stats->total_edges = b->total_edges;
+        stats->rounds_max = rmax;
+        stats->rounds_sum = rsum;
+        stats->lifts = (int64_t)c.lifts;
+        stats->edges = (int64_t)c.edges;
+        stats->num_top = (int64_t)c.num_top;
+        stats->solve_ms = ms;
+        stats->block = b->block;
+        stats->grid = grid;
+        stats->games_failed = failed;
+        stats->graph_replayed = replay ? 1 : 0;
+    }
+    if (first != EG_OK) return eg_set_error(first, "%d game(s) stopped early (status %d)", failed, (int)first);
+    return EG_OK;
+}
+
+extern "C" eg_status eg_batch_credits(eg_batch *b, int32_t game, int64_t *credits)
+{
+    if (!b || !credits || game < 0 || game >= b->num_games) return eg_set_error(EG_ERR_INVALID, "bad arguments");
+    if (!b->solved) return eg_set_error(EG_ERR_INVALID, "batch not solved");
+    EG_CUDA(cudaSetDevice(b->device));
+    const long long base = b->node_off_h[game], n = b->node_off_h[game + 1] - base;
+    std::vector<long long> rows((size_t)(n * b->K));
+    EG_CUDA(cudaMemcpyAsync(rows.data(), b->F + base * b->K, sizeof(long long) * rows.size(), cudaMemcpyDeviceToHost, b->st));
+    EG_CUDA(cudaStreamSynchronize(b->st));
+    for (long long v = 0; v < n; v++)
+        for (int k = 0; k < b->K; k++) credits[(size_t)k * n + v] = rows[(size_t)(v * b->K + k)];
+    return EG_OK;
+}
+
+extern "C" eg_status eg_batch_game_result(eg_batch *b, int32_t game, int64_t *rounds, int32_t *status)
+{
+    if (!b || game < 0 || game >= b->num_games) return eg_set_error(EG_ERR_INVALID, "bad arguments");
+    EG_CUDA(cudaSetDevice(b->device));
+    long long r = 0;
+    int s = 0;
+    EG_CUDA(cudaMemcpyAsync(&r, b->rounds + game, sizeof r, cudaMemcpyDeviceToHost, b->st));
+    EG_CUDA(cudaMemcpyAsync(&s, b->status + game, sizeof s, cudaMemcpyDeviceToHost, b->st));
+    EG_CUDA(cudaStreamSynchronize(b->st));
+    if (rounds) *rounds = r;
+    if (status) *status = s;
+    return EG_OK;
+}
+
+/* Autotuner: each candidate CTA size solves the batch under a round cap
+ * (enough rounds to reach steady state, few enough to be quick); the one
+ * with the most edge relaxations per second is kept. */
+extern "C" eg_status eg_batch_tune(eg_batch *b, int32_t *block_out)
+{
+    if (!b) return eg_set_error(EG_ERR_INVALID, "batch is NULL");
+    if (!b->thresholds_set) return eg_set_error(EG_ERR_INVALID, "thresholds not set");
+    const int cands[] = {128, 256, 512, 1024};
+    const long long keep_cap = b->max_rounds;
+    const bool keep_graph = b->use_graph;
+    b->use_graph = false;
+    b->max_rounds = 64;
+    double best = -1.0;
+    int best_block = b->block;
+    for (int c : cands) {
+        b->block = c;
+        eg_batch_stats st;
+        eg_status s = eg_batch_solve(b, &st);
+        if (s != EG_OK && s != EG_ERR_LOOPCAP) continue;
+        const double rate = st.solve_ms > 0 ? (double)st.edges / st.solve_ms : 0.0;
+        if (rate > best) {
+            best = rate;
+            best_block = c;
+        }
+    }
+    b->block = best_block;
+    b->max_rounds = keep_cap;
+    b->use_graph = keep_graph;
+    b->solved = false;
+    if (block_out) *block_out = best_block;
+    if (best < 0) return eg_set_error(EG_ERR_CUDA, "no candidate CTA size ran");
+    return EG_OK;
+}

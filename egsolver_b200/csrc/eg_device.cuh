@@ -66,6 +66,16 @@ __device__ __forceinline__ bool bitmap_push(uint32_t *bm, int32_t p)
     return !(atomicOr(w, mask) & mask);
 }
 
+/* Sets bit p of a frontier bitmap without waiting for the old word (a
+ * reduction, not a fetch): the caller decides "the next round has work"
+ * from the raise itself, so the atomic's latency is off the critical path. */
+__device__ __forceinline__ void bitmap_mark(uint32_t *bm, int32_t p)
+{
+    const uint32_t mask = 1u << (p & 31);
+    uint32_t *w = bm + (p >> 5);
+    if (!(__ldcg(w) & mask)) atomicOr(w, mask);
+}
+
 /* Control block of a persistent solve.  Counters that a round uses are
  * double-buffered by round parity and cleared by the barrier's last
  * arriver, so that no extra pass over them is needed. */
@@ -82,6 +92,8 @@ struct Ctrl {
     unsigned long long t_start;        /* globaltimer at kernel start                */
     unsigned long long wait_site;      /* diagnostic: round at which a wait gave up  */
     unsigned long long num_top;        /* vertices at TOP after the solve            */
+    unsigned long long changes;        /* lifts that raised a credit                 */
+    unsigned long long pushes;         /* predecessor entries scanned                */
 };
 
 /* Grid barrier for a cooperative launch.  Every wait is bounded by

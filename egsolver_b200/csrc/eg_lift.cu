@@ -59,6 +59,17 @@ __device__ __forceinline__ int64_t shfl_xor<int64_t>(unsigned mask, int64_t v, i
     return (int64_t)__shfl_xor_sync(mask, (long long)v, off, width);
 }
 
+template <class T>
+__device__ __forceinline__ T shfl_idx(unsigned mask, T v, int src, int width)
+{
+    return __shfl_sync(mask, v, src, width);
+}
+template <>
+__device__ __forceinline__ int64_t shfl_idx<int64_t>(unsigned mask, int64_t v, int src, int width)
+{
+    return (int64_t)__shfl_sync(mask, (long long)v, src, width);
+}
+
 /* Position of the k-th (0-based) set bit of w; requires popc(w) > k. */
 __device__ __forceinline__ int nth_set_bit(uint32_t w, int k)
 {
@@ -78,34 +89,62 @@ __device__ __forceinline__ int nth_set_bit(uint32_t w, int k)
     return pos;
 }
 
+/* Where pushes go and how credits are read: the persistent grid kernel
+ * marks a global bitmap and reads credits from L2; the single-CTA kernel
+ * owns its game, marks a shared-memory bitmap and may cache credits in L1. */
+struct GridPolicy {
+    uint32_t *bm;
+    __device__ __forceinline__ void push(int32_t p) const { bitmap_mark(bm, p); }
+    template <class T> __device__ __forceinline__ T load(const T *a) const { return ld_credit(a); }
+    template <class T> __device__ __forceinline__ void store(T *a, T v) const { st_credit(a, v); }
+};
+struct CtaPolicy {
+    uint32_t *bm; /* shared memory */
+    __device__ __forceinline__ void push(int32_t p) const { atomicOr(bm + (p >> 5), 1u << (p & 31)); }
+    template <class T> __device__ __forceinline__ T load(const T *a) const { return *a; }
+    template <class T> __device__ __forceinline__ void store(T *a, T v) const { *a = v; }
+};
+
 struct LiftCounters {
     unsigned long long lifts, edges;
+    unsigned changes, pushes;
     int any_new;
 };
 
 /* Lift vertex u with the G lanes of one group (gl = lane in group). */
-template <class T, int G, int OWNER>
-__device__ __forceinline__ void lift_group(const LiftParams &p, T *F, uint32_t *nxt, int u, int gl, unsigned gmask,
+template <class T, int G, int OWNER, class Pol>
+__device__ __forceinline__ void lift_group(const LiftParams &p, T *F, const Pol &pol, int u, int gl, unsigned gmask,
                                            LiftCounters &cnt)
 {
     const int b = __ldg(p.P + u) >> 1, e = __ldg(p.P + u + 1) >> 1;
+    /* Only the group leader reads the old credit, before the reduction (a
+     * group-wide synchronisation point) and so before its own write below:
+     * a lane that read F[u] after the leader's write would see no change and
+     * skip its share of the predecessor pushes. */
+    T old = (gl == 0) ? pol.load(F + u) : (T)0;
     T acc = identity<OWNER, T>();
     int real = 0;
     for (int k = b + gl; k < e; k += G) {
         const int4 q = __ldg(p.E4 + k);
-        const T v0 = ominus<T>(ld_credit(F + q.x), q.y, p.mg);
-        const T v1 = ominus<T>(ld_credit(F + q.z), q.w, p.mg);
+        const T v0 = ominus<T>(pol.load(F + q.x), q.y, p.mg);
+        const T v1 = ominus<T>(pol.load(F + q.z), q.w, p.mg);
         acc = combine<OWNER>(acc, combine<OWNER>(v0, v1));
         real += 1 + (q.z < p.n_pad);
     }
 #pragma unroll
     for (int off = G / 2; off > 0; off >>= 1) acc = combine<OWNER>(acc, shfl_xor<T>(gmask, acc, off, G));
+    if (G > 1) old = shfl_idx<T>(gmask, old, 0, G);
     cnt.edges += (unsigned long long)real;
-    const T old = ld_credit(F + u);
     if (old < acc) {
-        if (gl == 0) st_credit(F + u, acc);
+        if (gl == 0) {
+            pol.store(F + u, acc);
+            cnt.changes++;
+        }
         const int cb = __ldg(p.CP + u), ce = __ldg(p.CP + u + 1);
-        for (int k = cb + gl; k < ce; k += G) cnt.any_new |= bitmap_push(nxt, __ldg(p.CS + k));
+        if (gl == 0) cnt.pushes += (unsigned)(ce - cb);
+        cnt.any_new |= ce > cb;
+#pragma unroll 4
+        for (int k = cb + gl; k < ce; k += G) pol.push(__ldg(p.CS + k));
     }
     if (gl == 0) cnt.lifts++;
 }
@@ -121,6 +160,7 @@ __device__ __noinline__ void warp_class(const LiftParams &p, const LiftClass &lc
     constexpr int NG = 32 / G;
     const int grp = lane / G, gl = lane % G;
     const unsigned gmask = (G == 32) ? 0xffffffffu : (((1u << G) - 1u) << (grp * G));
+    const GridPolicy pol{nxt};
     for (;;) {
         int w0 = 0;
         if (lane == 0) w0 = atomicAdd(ctr, lc.grab);
@@ -137,17 +177,87 @@ __device__ __noinline__ void warp_class(const LiftParams &p, const LiftClass &lc
             word = __shfl_sync(0xffffffffu, word, 0);
             const int base_u = gw << 5;
             if (G == 1) {
-                if ((word >> lane) & 1u) lift_group<T, 1, OWNER>(p, F, nxt, base_u + lane, 0, 0u, cnt);
+                if ((word >> lane) & 1u) lift_group<T, 1, OWNER>(p, F, pol, base_u + lane, 0, 0u, cnt);
             } else {
                 while (word) {
                     const int c = __popc(word);
-                    if (grp < c) lift_group<T, G, OWNER>(p, F, nxt, base_u + nth_set_bit(word, grp), gl, gmask, cnt);
+                    if (grp < c) lift_group<T, G, OWNER>(p, F, pol, base_u + nth_set_bit(word, grp), gl, gmask, cnt);
                     if (c <= NG) {
                         word = 0;
                     } else {
                         const int last = nth_set_bit(word, NG - 1);
                         word &= ~((2u << last) - 1u);
                     }
+                }
+            }
+        }
+    }
+}
+
+/* Thread-per-vertex processing with memory-level parallelism: a warp takes
+ * U consecutive frontier words at a time (static assignment over the grid,
+ * so no counter is touched) and every lane carries the U vertices it owns in
+ * those words through each load phase together. */
+template <class T, int OWNER>
+__device__ __noinline__ void thread_class(const LiftParams &p, const LiftClass &lc, T *F, uint32_t *cur, uint32_t *nxt,
+                                          LiftCounters &cnt)
+{
+    constexpr int U = 4;
+    const int lane = threadIdx.x & 31;
+    const int gwarp = (int)((blockIdx.x * (unsigned)blockDim.x + threadIdx.x) >> 5);
+    const int nwarp = (int)((gridDim.x * (unsigned)blockDim.x) >> 5);
+    const int nwords = lc.word_end - lc.word_begin;
+    for (int w0 = gwarp * U; w0 < nwords; w0 += nwarp * U) {
+        uint32_t mine = 0;
+        if (lane < U && w0 + lane < nwords) {
+            uint32_t *wp = cur + lc.word_begin + w0 + lane;
+            mine = __ldcg(wp);
+            if (mine) __stcg(wp, 0u);
+        }
+        int u[U], b[U], e[U];
+        T old[U], acc[U];
+#pragma unroll
+        for (int j = 0; j < U; j++) {
+            const uint32_t wj = __shfl_sync(0xffffffffu, mine, j);
+            u[j] = ((lc.word_begin + w0 + j) << 5) + lane;
+            acc[j] = identity<OWNER, T>();
+            b[j] = e[j] = 0;
+            old[j] = 0;
+            if ((wj >> lane) & 1u) {
+                b[j] = __ldg(p.P + u[j]) >> 1;
+                e[j] = __ldg(p.P + u[j] + 1) >> 1;
+                old[j] = ld_credit(F + u[j]);
+            }
+        }
+        int real = 0;
+        for (int k = 0;; k++) {
+            bool more = false;
+#pragma unroll
+            for (int j = 0; j < U; j++) {
+                if (b[j] + k < e[j]) {
+                    const int4 q = __ldg(p.E4 + b[j] + k);
+                    const T v0 = ominus<T>(ld_credit(F + q.x), q.y, p.mg);
+                    const T v1 = ominus<T>(ld_credit(F + q.z), q.w, p.mg);
+                    acc[j] = combine<OWNER>(acc[j], combine<OWNER>(v0, v1));
+                    real += 1 + (q.z < p.n_pad);
+                    more = true;
+                }
+            }
+            if (!more) break;
+        }
+        cnt.edges += (unsigned long long)real;
+#pragma unroll
+        for (int j = 0; j < U; j++) {
+            if (e[j] > b[j]) {
+                cnt.lifts++;
+                if (old[j] < acc[j]) {
+                    st_credit(F + u[j], acc[j]);
+                    cnt.changes++;
+                    const int cb = __ldg(p.CP + u[j]), ce = __ldg(p.CP + u[j] + 1);
+                    cnt.pushes += (unsigned)(ce - cb);
+                    cnt.any_new |= ce > cb;
+#pragma unroll 4
+                    for (int k = cb; k < ce; k++) bitmap_mark(nxt, __ldg(p.CS + k));
                 }
             }
         }
@@ -162,6 +272,7 @@ __device__ __noinline__ void cta_class(const LiftParams &p, const LiftClass &lc,
     __shared__ int s_w;
     __shared__ uint32_t s_word;
     __shared__ T s_red[LIFT_BLOCK / 32];
+    __shared__ int s_raise;
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     const int nwords = lc.word_end - lc.word_begin;
     for (;;) {
@@ -203,15 +314,24 @@ __device__ __noinline__ void cta_class(const LiftParams &p, const LiftClass &lc,
                 T x = lane < LIFT_BLOCK / 32 ? s_red[lane] : identity<OWNER, T>();
 #pragma unroll
                 for (int off = 16; off > 0; off >>= 1) x = combine<OWNER>(x, shfl_xor<T>(0xffffffffu, x, off, 32));
-                if (lane == 0) s_red[0] = x;
+                if (lane == 0) {
+                    /* one thread reads, compares and writes, so that no thread
+                     * can read the credit after it was raised */
+                    const T old = ld_credit(F + u);
+                    const int raise = old < x;
+                    if (raise) st_credit(F + u, x);
+                    s_raise = raise;
+                }
             }
             __syncthreads();
-            acc = s_red[0];
-            const T old = ld_credit(F + u);
-            if (old < acc) {
-                if (threadIdx.x == 0) st_credit(F + u, acc);
+            if (s_raise) {
                 const int cb = __ldg(p.CP + u), ce = __ldg(p.CP + u + 1);
-                for (int k = cb + threadIdx.x; k < ce; k += LIFT_BLOCK) cnt.any_new |= bitmap_push(nxt, __ldg(p.CS + k));
+                if (threadIdx.x == 0) {
+                    cnt.changes++;
+                    cnt.pushes += (unsigned)(ce - cb);
+                }
+                cnt.any_new |= ce > cb;
+                for (int k = cb + threadIdx.x; k < ce; k += LIFT_BLOCK) bitmap_mark(nxt, __ldg(p.CS + k));
             }
             if (threadIdx.x == 0) cnt.lifts++;
             __syncthreads();
@@ -225,7 +345,7 @@ __device__ __forceinline__ void run_class(const LiftParams &p, const LiftClass &
 {
     switch (lc.group) {
     case EG_GROUP_CTA: cta_class<T, OWNER>(p, lc, F, cur, nxt, ctr, cnt); break;
-    case 1: warp_class<T, 1, OWNER>(p, lc, F, cur, nxt, ctr, cnt); break;
+    case 1: thread_class<T, OWNER>(p, lc, F, cur, nxt, cnt); break;
     case 2: warp_class<T, 2, OWNER>(p, lc, F, cur, nxt, ctr, cnt); break;
     case 4: warp_class<T, 4, OWNER>(p, lc, F, cur, nxt, ctr, cnt); break;
     case 8: warp_class<T, 8, OWNER>(p, lc, F, cur, nxt, ctr, cnt); break;
@@ -239,7 +359,7 @@ __global__ void __launch_bounds__(LIFT_BLOCK, 2) k_lift(const __grid_constant__ 
 {
     Ctrl *c = p.ctrl;
     T *F = (T *)p.F;
-    LiftCounters cnt = {0ull, 0ull, 0};
+    LiftCounters cnt = {0ull, 0ull, 0u, 0u, 0};
     if (blockIdx.x == 0 && threadIdx.x == 0) c->t_start = globaltimer_ns();
     for (long long round = 0;; round++) {
         uint32_t *cur = (round & 1) ? p.B1 : p.B0;
@@ -273,16 +393,151 @@ __global__ void __launch_bounds__(LIFT_BLOCK, 2) k_lift(const __grid_constant__ 
         if (!ld_volatile(&c->flag[(round + 1) & 1])) break;
     }
     /* statistics */
-    unsigned long long l = cnt.lifts, e = cnt.edges;
+    unsigned long long l = cnt.lifts, e = cnt.edges, ch = cnt.changes, pu = cnt.pushes;
 #pragma unroll
     for (int off = 16; off > 0; off >>= 1) {
         l += __shfl_xor_sync(0xffffffffu, l, off);
         e += __shfl_xor_sync(0xffffffffu, e, off);
+        ch += __shfl_xor_sync(0xffffffffu, ch, off);
+        pu += __shfl_xor_sync(0xffffffffu, pu, off);
     }
     if ((threadIdx.x & 31) == 0) {
         atomicAdd(&c->lifts, l);
         atomicAdd(&c->edges, e);
+        atomicAdd(&c->changes, ch);
+        atomicAdd(&c->pushes, pu);
     }
+}
+
+/* One CTA of the shared-memory kernel: warps take words of a class from a
+ * shared counter and serve them with G lanes per vertex (1, or 8 / 32 for
+ * the larger buckets). */
+template <class T, int G, int OWNER>
+__device__ __forceinline__ void cta_warp_class(const LiftParams &p, const LiftClass &lc, T *F, uint32_t *cur,
+                                               const CtaPolicy &pol, int *ctr, LiftCounters &cnt)
+{
+    const int lane = threadIdx.x & 31;
+    constexpr int NG = 32 / G;
+    const int grp = lane / G, gl = lane % G;
+    const unsigned gmask = (G == 32) ? 0xffffffffu : (((1u << G) - 1u) << (grp * G));
+    const int nwords = lc.word_end - lc.word_begin;
+    for (;;) {
+        int wi = 0;
+        if (lane == 0) wi = atomicAdd(ctr, 1);
+        wi = __shfl_sync(0xffffffffu, wi, 0);
+        if (wi >= nwords) break;
+        const int gw = lc.word_begin + wi;
+        uint32_t word = cur[gw];
+        __syncwarp();
+        if (lane == 0 && word) cur[gw] = 0;
+        const int base_u = gw << 5;
+        if (G == 1) {
+            if ((word >> lane) & 1u) lift_group<T, 1, OWNER>(p, F, pol, base_u + lane, 0, 0u, cnt);
+            continue;
+        }
+        while (word) {
+            const int c = __popc(word);
+            if (grp < c) lift_group<T, G, OWNER>(p, F, pol, base_u + nth_set_bit(word, grp), gl, gmask, cnt);
+            if (c <= NG) {
+                word = 0;
+            } else {
+                const int last = nth_set_bit(word, NG - 1);
+                word &= ~((2u << last) - 1u);
+            }
+        }
+    }
+}
+
+/* A whole small game lifted by one CTA: both frontier bitmaps in shared
+ * memory, rounds separated by __syncthreads, termination by
+ * __syncthreads_or; no grid barrier and no spin-wait at all. */
+template <class T>
+__global__ void __launch_bounds__(1024, 1) k_lift_cta(const __grid_constant__ LiftParams p)
+{
+    extern __shared__ uint32_t sbits[];
+    __shared__ int s_ctr[2][EG_MAX_CLASSES];
+    const int words = p.n_pad >> 5;
+    uint32_t *cur = sbits, *nxt = sbits + words;
+    T *F = (T *)p.F;
+    Ctrl *c = p.ctrl;
+    LiftCounters cnt = {0ull, 0ull, 0u, 0u, 0};
+    for (int w = threadIdx.x; w < words; w += blockDim.x) {
+        cur[w] = p.B0[w];
+        nxt[w] = 0;
+    }
+    if (threadIdx.x < 2 * EG_MAX_CLASSES) (&s_ctr[0][0])[threadIdx.x] = 0;
+    const unsigned long long t0 = globaltimer_ns();
+    __syncthreads();
+    long long round = 0;
+    int stop = 0;
+    for (;;) {
+        if (threadIdx.x < EG_MAX_CLASSES) s_ctr[(round + 1) & 1][threadIdx.x] = 0;
+        cnt.any_new = 0;
+        const CtaPolicy pol{nxt};
+        for (int ci = 0; ci < p.nclasses; ci++) {
+            const LiftClass &lc = p.cls[ci];
+            int *ctr = &s_ctr[round & 1][ci];
+            const int g = lc.group;
+            if (lc.owner) {
+                if (g == 1) cta_warp_class<T, 1, 1>(p, lc, F, cur, pol, ctr, cnt);
+                else if (g == 8) cta_warp_class<T, 8, 1>(p, lc, F, cur, pol, ctr, cnt);
+                else cta_warp_class<T, 32, 1>(p, lc, F, cur, pol, ctr, cnt);
+            } else {
+                if (g == 1) cta_warp_class<T, 1, 0>(p, lc, F, cur, pol, ctr, cnt);
+                else if (g == 8) cta_warp_class<T, 8, 0>(p, lc, F, cur, pol, ctr, cnt);
+                else cta_warp_class<T, 32, 0>(p, lc, F, cur, pol, ctr, cnt);
+            }
+        }
+        round++;
+        if (!__syncthreads_or(cnt.any_new)) break;
+        if (p.max_rounds >= 0 && round >= p.max_rounds) {
+            stop = EG_ERR_LOOPCAP;
+            break;
+        }
+        const int late = __syncthreads_or(threadIdx.x == 0 && ((((round - 1) & 63) == 0 && p.cancel && ld_volatile(p.cancel)) ? 2 :
+                                           (p.timeout_ns && globaltimer_ns() - t0 > p.timeout_ns) ? 1 : 0));
+        if (late) {
+            /* distinguish cancel from timeout with one more vote */
+            const int was_cancel = __syncthreads_or(threadIdx.x == 0 && p.cancel && ld_volatile(p.cancel));
+            stop = was_cancel ? EG_ERR_CANCELLED : EG_ERR_TIMEOUT;
+            break;
+        }
+        uint32_t *t = cur;
+        cur = nxt;
+        nxt = t;
+    }
+    unsigned long long l = cnt.lifts, e = cnt.edges, ch = cnt.changes, pu = cnt.pushes;
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) {
+        l += __shfl_xor_sync(0xffffffffu, l, off);
+        e += __shfl_xor_sync(0xffffffffu, e, off);
+        ch += __shfl_xor_sync(0xffffffffu, ch, off);
+        pu += __shfl_xor_sync(0xffffffffu, pu, off);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        atomicAdd(&c->lifts, l);
+        atomicAdd(&c->edges, e);
+        atomicAdd(&c->changes, ch);
+        atomicAdd(&c->pushes, pu);
+    }
+    if (threadIdx.x == 0) {
+        c->rounds = round;
+        c->stop = stop;
+    }
+}
+
+eg_status launch_lift_cta(const LiftParams &p, int credit_bits, cudaStream_t st)
+{
+    const void *fn = credit_bits == 32 ? (const void *)k_lift_cta<int32_t> : (const void *)k_lift_cta<int64_t>;
+    const size_t smem = (size_t)(p.n_pad / 32) * 2 * sizeof(uint32_t);
+    cudaError_t err = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (err != cudaSuccess)
+        return eg_set_error(EG_ERR_CUDA, "shared-memory kernel does not fit (%zu B): %s", smem, cudaGetErrorString(err));
+    void *args[] = {(void *)&p};
+    err = cudaLaunchKernel(fn, dim3(1), dim3(1024), args, smem, st);
+    if (err != cudaSuccess)
+        return eg_set_error(EG_ERR_CUDA, "launch of the shared-memory kernel failed: %s", cudaGetErrorString(err));
+    return EG_OK;
 }
 
 eg_status launch_lift(const LiftParams &p, int credit_bits, cudaStream_t st, int *grid, int *block)

@@ -40,6 +40,8 @@ struct LiftParams {
 /* Cooperative launch of the persistent lifting kernel on `st`; *grid gets
  * the number of CTAs used. */
 eg_status launch_lift(const LiftParams &p, int credit_bits, cudaStream_t st, int *grid, int *block);
+/* One-CTA launch for small games (frontier in shared memory). */
+eg_status launch_lift_cta(const LiftParams &p, int credit_bits, cudaStream_t st);
 
 }  // namespace eg
 

@@ -24,3 +24,21 @@ def cfg2(n: int = 1 << 20):
 
 def cfg3(n: int = 2000):
     return generate(3, n, n - 1, 500, SEED + 3)
+
+
+def cfg4_games(num_games: int = 4096, seed: int = SEED + 4):
+    """Batched workload: games with n log-uniform in [1024, 65536], out-degree
+    uniform in {2..16}, owners 50/50, weights uniform in [-100, 100]."""
+    import numpy as np
+
+    rng = np.random.default_rng(seed)
+    ns = np.rint(np.exp(rng.uniform(np.log(1024), np.log(65536), num_games))).astype(int)
+    return [generate(4, int(n), 16, 100, seed * 1_000_003 + i, param=2) for i, n in enumerate(ns)]
+
+
+def cfg4_thresholds(num_games: int = 4096, k: int = 8, seed: int = SEED + 4):
+    """K = 8 mean-payoff thresholds p/d per game, d = 8, p uniform in [-800, 800]."""
+    import numpy as np
+
+    rng = np.random.default_rng(seed + 1)
+    return rng.integers(-800, 801, size=(num_games, k)).astype(np.int32), 8

@@ -114,7 +114,10 @@ typedef struct eg_stats {
     int32_t credit_bits;         /* width actually used                               */
     int32_t variant_small, variant_mid, variant_large; /* variants used per bucket   */
     int32_t small_max_deg, large_min_deg;               /* bucket bounds used         */
-    int32_t reserved[4];
+    int64_t changes;             /* lifts that raised a credit                        */
+    int64_t pushes;              /* predecessor entries scanned after those raises    */
+    int32_t grid, block;         /* launch shape of the lifting kernel                */
+    int32_t reserved[2];
 } eg_stats;
 
 /* ------------------------------------------------------------------ */
@@ -197,6 +200,61 @@ void eg_dgame_free(eg_dgame *g);
 eg_status eg_csr2csc_i32(int32_t num_rows, int32_t num_cols, int64_t nnz,
                          const int64_t *row_ptr, const int32_t *col_idx, const int32_t *val,
                          int64_t *csc_ptr, int32_t *csc_row, int32_t *csc_val);
+
+/* ------------------------------------------------------------------ */
+/* Batched solving: many games x K thresholds in one persistent launch  */
+/* ------------------------------------------------------------------ */
+
+/* A mean-payoff query "is the mean payoff of v at least p/d?" is the
+ * energy game with weights w*d - p (new; the reference solves one energy
+ * game per process).  A batch packs many games into one device-resident
+ * multi-CSR that their CSC, owners and credits share; one persistent kernel
+ * then solves every (game, threshold) pair, one game per CTA with its K
+ * thresholds on K lanes, games taken from a device queue largest first. */
+#define EG_BATCH_MAX_K 32
+
+typedef struct eg_batch eg_batch;
+
+typedef struct eg_batch_opts {
+    int32_t thresholds;          /* K thresholds per game, 1..EG_BATCH_MAX_K        */
+    int32_t scale;               /* d >= 1: threshold p turns w into w*d - p        */
+    int32_t block;               /* threads per CTA (128..1024); 0 = autotuned      */
+    int32_t device;
+    int64_t max_rounds;          /* per game; < 0: no cap                           */
+    double  timeout_ms;          /* per launch; <= 0: none                          */
+    int32_t use_graph;           /* non-zero: the solve's launches are captured in a
+                                    CUDA graph on the first solve and replayed      */
+    int32_t reserved[7];
+} eg_batch_opts;
+
+typedef struct eg_batch_stats {
+    int32_t num_games, thresholds;
+    int64_t total_nodes, total_edges;
+    int64_t rounds_max, rounds_sum;  /* over games                                   */
+    int64_t lifts;                   /* vertex lifts (all K thresholds at once)       */
+    int64_t edges;                   /* edge relaxations summed over the K thresholds */
+    int64_t num_top;                 /* (vertex, threshold) pairs at TOP              */
+    double  solve_ms;                /* device time of the launch                     */
+    int32_t block, grid, games_failed, graph_replayed;
+    int32_t reserved[4];
+} eg_batch_stats;
+
+/* Packs and uploads the games (each in eg_game form; all at most 2^19
+ * vertices) and builds their CSC on the device. */
+eg_status eg_batch_create(const eg_game *games, int32_t num_games, const eg_batch_opts *opts, eg_batch **out);
+/* Thresholds p[g*K + k] for every game g and threshold k. */
+eg_status eg_batch_set_thresholds(eg_batch *b, const int32_t *p);
+/* Solves every (game, threshold); credits stay on the device. */
+eg_status eg_batch_solve(eg_batch *b, eg_batch_stats *stats);
+/* Credits of one game, threshold-major: credits[k * n_g + v] (TOP = EG_TOP64). */
+eg_status eg_batch_credits(eg_batch *b, int32_t game, int64_t *credits);
+/* Per-game outcome of the last solve: rounds and an eg_status. */
+eg_status eg_batch_game_result(eg_batch *b, int32_t game, int64_t *rounds, int32_t *status);
+/* Autotuner: times the candidate CTA sizes on the batch's largest games and
+ * keeps the fastest for later solves (*block receives it). */
+eg_status eg_batch_tune(eg_batch *b, int32_t *block);
+int64_t eg_batch_device_bytes(const eg_batch *b);
+void eg_batch_free(eg_batch *b);
 
 /* ------------------------------------------------------------------ */
 /* Cancellation                                                         */

@@ -1,0 +1,103 @@
+"""GPU parity of the batched solver: every (game, threshold) of a batch equals
+the oracle's solve of the energy game with weights w*d - p."""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+import egsolver_b200 as eg
+from egsolver_b200 import workloads
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+
+def small_batch(num=18, seed=5):
+    rng = np.random.default_rng(seed)
+    games = []
+    for i in range(num):
+        n = int(rng.integers(40, 1500))
+        kind = [1, 2, 4, 5][i % 4]
+        deg = {1: 3, 2: min(n - 1, 64), 4: 16, 5: 30}[kind]
+        games.append(eg.generate(kind, n, deg, int(rng.integers(3, 60)), 77 + i, param=2 if kind == 4 else 6))
+    return games
+
+
+def check_batch(b, games, p, d):
+    for g, game in enumerate(games):
+        got = b.credits(g)
+        for k in range(p.shape[1]):
+            want, st = O.eg_solve(eg.threshold_game(game, int(p[g, k]), d), bits=64)
+            assert st["finished"]
+            np.testing.assert_array_equal(got[k], want, err_msg=f"game {g} threshold {k} (p={p[g, k]})")
+
+
+@pytest.mark.parametrize("K", [1, 3, 8, 32])
+def test_small_batch_all_thresholds(K):
+    games = small_batch()
+    rng = np.random.default_rng(K)
+    d = 4
+    p = rng.integers(-60, 61, size=(len(games), K)).astype(np.int32)
+    with eg.Batch(games, thresholds=K, scale=d) as b:
+        b.set_thresholds(p)
+        _, st = b.solve()
+        assert st.games_failed == 0 and st.num_games == len(games)
+        check_batch(b, games, p, d)
+
+
+def test_cfg4_games_subset():
+    games = [g for g in workloads.cfg4_games(64) if g.num_nodes <= 2600][:6]
+    p_all, d = workloads.cfg4_thresholds(64)
+    p = p_all[: len(games)]
+    with eg.Batch(games, thresholds=8, scale=d) as b:
+        b.set_thresholds(p)
+        _, st = b.solve()
+        assert st.edges > 0
+        check_batch(b, games, p, d)
+
+
+def test_graph_replay_with_new_thresholds():
+    games = small_batch(10, seed=9)
+    d = 2
+    with eg.Batch(games, thresholds=4, scale=d, use_graph=True) as b:
+        for rep in range(3):
+            p = np.random.default_rng(rep).integers(-30, 31, size=(len(games), 4)).astype(np.int32)
+            b.set_thresholds(p)
+            _, st = b.solve()
+            assert st.graph_replayed == (1 if rep > 0 else 0)
+            check_batch(b, games, p, d)
+
+
+def test_autotuner_then_solve():
+    games = small_batch(12, seed=2)
+    p = np.random.default_rng(1).integers(-40, 41, size=(len(games), 8)).astype(np.int32)
+    with eg.Batch(games, thresholds=8, scale=3) as b:
+        b.set_thresholds(p)
+        blk = b.tune()
+        assert blk in (128, 256, 512, 1024)
+        _, st = b.solve()
+        assert st.block == blk
+        check_batch(b, games, p, 3)
+
+
+def test_round_cap_marks_games():
+    games = [workloads.cfg1()]
+    p = np.array([[40]], dtype=np.int32)  # strongly negative weights: long climb to TOP
+    with eg.Batch(games, thresholds=1, scale=1, max_rounds=2) as b:
+        b.set_thresholds(p)
+        status, st = b.solve(raise_on_error=False)
+        assert eg._ffi.STATUS_NAMES[status] == "EG_ERR_LOOPCAP"
+        rounds, gst = b.game_result(0)
+        assert rounds == 2 and eg._ffi.STATUS_NAMES[gst] == "EG_ERR_LOOPCAP"
+
+
+def test_owner_arrays_in_a_batch():
+    g = workloads.cfg1(300)
+    own = g.owners().copy()
+    h = eg.Game(row_ptr=g.row_ptr, succ=g.succ, weight=g.weight, owner=own)
+    p = np.array([[0, 5], [0, 5]], dtype=np.int32)
+    with eg.Batch([g, h], thresholds=2, scale=1) as b:
+        b.set_thresholds(p)
+        b.solve()
+        np.testing.assert_array_equal(b.credits(0), b.credits(1))
+        check_batch(b, [g, h], p, 1)

@@ -1,0 +1,264 @@
+"""GPU parity: the CUDA solver, called through the C-ABI, against the oracle
+(bit-exact credits, TOP set and winning region) on golden fixtures, the
+benchmark configurations at oracle-friendly sizes, and edge cases."""
+from __future__ import annotations
+
+import subprocess
+
+import numpy as np
+import pytest
+
+import egsolver_b200 as eg
+from egsolver_b200 import workloads
+from oracle import oracle as O
+from tests.conftest import GOLDEN, ROOT, by_ext, load_solution, to_top32
+
+pytestmark = pytest.mark.gpu
+
+VARIANTS = [
+    dict(variant=eg.VARIANT_AUTO),
+    dict(variant=eg.VARIANT_THREAD),
+    dict(variant=eg.VARIANT_WARP, lanes_per_vertex=2),
+    dict(variant=eg.VARIANT_WARP, lanes_per_vertex=4),
+    dict(variant=eg.VARIANT_WARP, lanes_per_vertex=8),
+    dict(variant=eg.VARIANT_WARP, lanes_per_vertex=16),
+    dict(variant=eg.VARIANT_WARP, lanes_per_vertex=32),
+    dict(variant=eg.VARIANT_CTA),
+    dict(variant=eg.VARIANT_SMEM),
+]
+
+
+def vid(v):
+    return "-".join(f"{k}{x}" for k, x in v.items())
+
+
+def assert_exact(game, gpu: np.ndarray, bits: int):
+    ref, st = O.eg_solve(game, bits=64)
+    assert st["finished"]
+    if bits == 32:
+        np.testing.assert_array_equal(gpu.astype(np.int64), to_top32(ref))
+    else:
+        np.testing.assert_array_equal(gpu, ref)
+    # winning region of player 0 = finite credits
+    np.testing.assert_array_equal(gpu < (2**31 - 1 if bits == 32 else 2**63 - 1), ref < O.TOP64)
+
+
+@pytest.mark.parametrize("v", VARIANTS, ids=vid)
+@pytest.mark.parametrize("bits", [32, 64])
+def test_fig2_known_answer(golden_fig2, v, bits):
+    game, sol = golden_fig2
+    f, st = eg.solve(game, credit_bits=bits, **v)
+    assert by_ext(game, to_top32(f) if bits == 64 else f) == sol
+    assert st.mg == 7
+
+
+@pytest.mark.parametrize("v", [VARIANTS[0], VARIANTS[6], VARIANTS[7], VARIANTS[1], VARIANTS[8]], ids=vid)
+def test_golden_clique_500_cp4(golden_clique, v):
+    game, sol = golden_clique
+    f, st = eg.solve(game, credit_bits=32, **v)
+    assert by_ext(game, f) == sol
+    assert st.num_top == 1000
+    assert st.mg == 1992
+
+
+@pytest.mark.parametrize("v", VARIANTS, ids=vid)
+def test_cfg1_all_variants(v):
+    game = workloads.cfg1()
+    for bits in (32, 64):
+        f, st = eg.solve(game, credit_bits=bits, **v)
+        assert_exact(game, f, bits)
+        assert st.edges >= st.lifts * 4
+
+
+@pytest.mark.parametrize("v", [VARIANTS[0], VARIANTS[5], VARIANTS[6], VARIANTS[7]], ids=vid)
+def test_cfg3_clique_2000(v):
+    game = workloads.cfg3()
+    f, _ = eg.solve(game, credit_bits=32, **v)
+    assert_exact(game, f, 32)
+
+
+@pytest.mark.parametrize("n", [1 << 12, 1 << 14])
+def test_cfg2_scaled_int64(n):
+    game = workloads.cfg2(n)
+    f, st = eg.solve(game, credit_bits=64)
+    assert_exact(game, f, 64)
+    assert st.rounds > 1
+
+
+def test_cfg2_scaled_variants_and_buckets():
+    game = workloads.cfg2(1 << 12)
+    ref, _ = O.eg_solve(game, bits=64)
+    for v in VARIANTS[1:] + [dict(small_max_deg=2, large_min_deg=40), dict(small_max_deg=64, large_min_deg=65)]:
+        f, _ = eg.solve(game, credit_bits=64, **v)
+        np.testing.assert_array_equal(f, ref, err_msg=str(v))
+
+
+def test_random_small_games_bit_exact():
+    kinds = [(1, 3), (2, 60), (4, 16), (5, 40)]
+    for seed in range(12):
+        kind, deg = kinds[seed % 4]
+        g = eg.generate(kind, 64 + 37 * seed, deg, 3 + 5 * seed, 1000 + seed, param=2 if kind == 4 else 5)
+        for v in (VARIANTS[0], VARIANTS[1], VARIANTS[4], VARIANTS[7], VARIANTS[8]):
+            f, _ = eg.solve(g, credit_bits=64, **v)
+            assert_exact(g, f, 64)
+
+
+def test_owner_array_equals_split_convention():
+    g = workloads.cfg1()
+    ref, _ = eg.solve(g)
+    # same game with vertices shuffled and owners given per vertex
+    rng = np.random.default_rng(3)
+    n = g.num_nodes
+    perm = rng.permutation(n)  # new -> old
+    inv = np.empty(n, np.int64)
+    inv[perm] = np.arange(n)
+    deg = np.diff(g.row_ptr)[perm]
+    rp = np.concatenate([[0], np.cumsum(deg)])
+    succ = np.concatenate([inv[g.succ[g.row_ptr[o]:g.row_ptr[o + 1]]] for o in perm]).astype(np.int32)
+    w = np.concatenate([g.weight[g.row_ptr[o]:g.row_ptr[o + 1]] for o in perm])
+    h = eg.Game(row_ptr=rp, succ=succ, weight=w, owner=g.owners()[perm])
+    f, _ = eg.solve(h)
+    np.testing.assert_array_equal(f, ref[perm])
+
+
+def test_single_vertex_self_loops():
+    # player 0 with only a negative self-loop: credit climbs past MG -> TOP
+    g = eg.Game(row_ptr=[0, 1], succ=[0], weight=[-1], num_nodes0=1)
+    f, st = eg.solve(g)
+    assert f[0] == eg.EG_TOP64 and st.mg == 1
+    # player 1 with a positive self-loop: credit 0
+    g = eg.Game(row_ptr=[0, 1], succ=[0], weight=[5], num_nodes0=0)
+    f, _ = eg.solve(g, credit_bits=32)
+    assert f[0] == 0
+
+
+def test_mg_beyond_int32_needs_64_bit_credits():
+    n = 4
+    w = [-(2**30), -(2**30), -(2**30), 7]
+    g = eg.Game(row_ptr=np.arange(n + 1), succ=[1, 2, 3, 0], weight=w, num_nodes0=2)
+    with pytest.raises(eg.EGError) as ei:
+        eg.solve(g, credit_bits=32)
+    assert ei.value.name == "EG_ERR_OVERFLOW"
+    f, st = eg.solve(g, credit_bits=64)
+    assert st.mg == 3 * 2**30
+    ref, _ = O.eg_solve(g, bits=64)
+    np.testing.assert_array_equal(f, ref)
+
+
+def test_sink_rejected():
+    g = eg.Game(row_ptr=[0, 1, 1], succ=[1], weight=[1], num_nodes0=1)
+    with pytest.raises(eg.EGError) as ei:
+        eg.solve(g)
+    assert ei.value.name == "EG_ERR_INVALID"
+
+
+def test_round_cap_gives_a_lower_bound():
+    g = workloads.cfg1()
+    ref, _ = O.eg_solve(g, bits=64)
+    with eg.ResidentGame(g) as r:
+        status, st = r.solve(raise_on_error=False, max_rounds=3)
+        assert eg._ffi.STATUS_NAMES[status] == "EG_ERR_LOOPCAP"
+        assert st.rounds == 3
+        part = r.credits()
+        assert np.all(part <= ref)
+        assert np.any(part < ref)
+
+
+def test_cancel_flag_stops_the_solve():
+    g = workloads.cfg2(1 << 14)
+    flag = eg.CancelFlag()
+    try:
+        flag.set(1)
+        with eg.ResidentGame(g) as r:
+            status, st = r.solve(raise_on_error=False, cancel=flag)
+            assert eg._ffi.STATUS_NAMES[status] == "EG_ERR_CANCELLED"
+            assert st.rounds == 1
+            flag.set(0)
+            status, _ = r.solve(raise_on_error=False, cancel=flag)
+            assert status == 0
+    finally:
+        flag.free()
+
+
+def test_timeout_stops_the_solve():
+    g = workloads.cfg2(1 << 14)
+    with eg.ResidentGame(g) as r:
+        status, st = r.solve(raise_on_error=False, timeout_ms=0.001)
+        assert eg._ffi.STATUS_NAMES[status] == "EG_ERR_TIMEOUT"
+        status, _ = r.solve(raise_on_error=False)
+        assert status == 0
+
+
+def test_resident_game_resolve_and_keep_layout():
+    g = workloads.cfg2(1 << 13)
+    ref, _ = O.eg_solve(g, bits=64)
+    with eg.ResidentGame(g) as r:
+        r.solve()
+        np.testing.assert_array_equal(r.credits(), ref)
+        _, st2 = r.solve(keep_layout=True)
+        np.testing.assert_array_equal(r.credits(), ref)
+        _, st3 = r.solve(credit_bits=32, keep_layout=True)
+        np.testing.assert_array_equal(r.credits(32).astype(np.int64), to_top32(ref))
+        assert st2.kernel_launches < st3.kernel_launches + 1
+        assert r.device_bytes > 0
+
+
+def test_from_device_pointers_with_torch():
+    torch = pytest.importorskip("torch")
+    g = workloads.cfg1()
+    ref, _ = eg.solve(g)
+    rp = torch.from_numpy(g.row_ptr).cuda()
+    sc = torch.from_numpy(g.succ).cuda()
+    wt = torch.from_numpy(g.weight).cuda()
+    r = eg.ResidentGame.from_device(g.num_nodes, g.num_edges, g.num_nodes0, rp.data_ptr(), sc.data_ptr(), wt.data_ptr())
+    r.solve()
+    ptr, bits = r.credits_device()
+    assert bits == 64 and ptr != 0
+    np.testing.assert_array_equal(r.credits(), ref)
+    r.free()
+
+
+def test_csr2csc_equals_host_csr2csc():
+    rng = np.random.default_rng(11)
+    for nrow, ncol, nnz in ((4, 5, 9), (100, 70, 3000), (2000, 5000, 100000), (9, 9, 0)):
+        counts = rng.multinomial(nnz, np.ones(nrow) / nrow)
+        rp = np.concatenate([[0], np.cumsum(counts)]).astype(np.int64)
+        col = rng.integers(0, ncol, nnz).astype(np.int32)
+        val = rng.integers(-1000, 1000, nnz).astype(np.int32)
+        got = eg.csr2csc(nrow, ncol, rp, col, val)
+        want = O.csr2csc(nrow, ncol, rp, col, val)
+        for a, b in zip(got, want):
+            np.testing.assert_array_equal(a, b)
+
+
+def test_csr2csc_of_cfg2_is_a_permutation_with_stable_columns():
+    g = workloads.cfg2(1 << 18)
+    cp, cr, cv = eg.csr2csc(g.num_nodes, g.num_nodes, g.row_ptr, g.succ, g.weight)
+    assert cp[-1] == g.num_edges
+    for c in range(0, g.num_nodes, 9973):  # rows ascending inside every column
+        seg = cr[cp[c]:cp[c + 1]]
+        assert np.all(np.diff(seg) >= 0)
+    want = O.csr2csc(g.num_nodes, g.num_nodes, g.row_ptr, g.succ, g.weight)
+    for a, b in zip((cp, cr, cv), want):
+        np.testing.assert_array_equal(a, b)
+
+
+@pytest.mark.skipif(not O.REF_BIN.exists(), reason="reference driver not built")
+@pytest.mark.parametrize("shuffling", ["1", "32"])
+def test_reference_driver_runs_unchanged_on_the_gpu(shuffling):
+    """The reference's own egsolver.c, linked against this library through the
+    reference-ABI shim, solves the golden game on the GPU."""
+    out = subprocess.run([str(O.REF_BIN), "--gpu", "--eg", "--shuffling", shuffling, "--input",
+                          str(GOLDEN / "clique_500_cp4.txt.gz")], capture_output=True, text=True, timeout=300,
+                         cwd=str(ROOT))
+    assert out.returncode == 0, out.stderr[-2000:]
+    sol = {}
+    seen = False
+    for line in out.stdout.splitlines():
+        if line.startswith("Solution:"):
+            seen = True
+            continue
+        if seen and ")" in line and line.split(")")[0].isdigit():
+            k, v = line.split(")")
+            sol[int(k)] = int(v)
+    assert sol == load_solution(GOLDEN / "clique_500_cp4.sol")
