@@ -55,7 +55,12 @@ def parse():
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=["cfg1", "cfg2", "cfg3"], default="cfg2")
+    ap.add_argument("--workload", choices=["cfg1", "cfg2", "cfg3", "cfg4", "cfg5"], default="cfg2")
+    ap.add_argument("--games", type=int, default=4096, help="cfg4: number of games")
+    ap.add_argument("--plain-sample", type=int, default=24, help="cfg4/cfg5: requests timed on the plain path")
+    ap.add_argument("--requests", type=int, default=200, help="cfg5: requests per arrival rate")
+    ap.add_argument("--rates", type=str, default="2,8,32,128", help="cfg5: arrival rates (requests/s) swept")
+    ap.add_argument("--n-max", type=int, default=1 << 19, help="cfg5: largest request game")
     ap.add_argument("--n", type=int, default=0, help="override the vertex count (smaller cases)")
     ap.add_argument("--e2e-steps", type=int, default=0, help="e2e steps (default: --steps)")
     ap.add_argument("--cpu-sample-s", type=float, default=10.0)
@@ -218,10 +223,139 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+def run_batched(args):
+    """cfg4: many uneven games x K=8 mean-payoff thresholds in one persistent
+    launch (CUDA-graph replay, autotuned CTA size) against the plain path that
+    launches the single-game solver once per (game, threshold)."""
+    import torch
+
+    import egsolver_b200 as eg
+    from egsolver_b200 import workloads
+
+    G = args.games
+    games = workloads.cfg4_games(G)
+    p, d = workloads.cfg4_thresholds(G)
+    K = p.shape[1]
+    t0 = time.perf_counter()
+    b = eg.Batch(games, thresholds=K, scale=d, use_graph=True)
+    b.set_thresholds(p)
+    setup_s = time.perf_counter() - t0
+    block = b.tune()
+    for _ in range(args.warmup):
+        b.solve()
+    sampler = ClockSampler(0)
+    times, stats = [], []
+    for _ in range(args.steps):
+        _, st = b.solve()
+        times.append(st.solve_ms)
+        stats.append(st)
+    clocks = sampler.stop()
+    ms = sum(times) / len(times)
+    value = G / (ms / 1e3)
+    # parity spot check on the checker: fixed point of a few transformed games
+    from oracle import oracle as O
+
+    rng = np.random.default_rng(0)
+    for g in rng.choice(G, size=min(8, G), replace=False):
+        cr = b.credits(int(g))
+        for k in range(K):
+            tg = eg.threshold_game(games[g], int(p[g, k]), d)
+            if O.count_inconsistent(tg, cr[k]) != 0:
+                raise RuntimeError(f"batched credits of game {g} threshold {k} are not a fixed point")
+    # plain path: one single-game solve per (game, threshold) on a seeded sample
+    pick = rng.choice(G, size=min(args.plain_sample, G), replace=False)
+    plain_ms, plain_pairs = 0.0, 0
+    for g in pick:
+        k = int(rng.integers(0, K))
+        tg = eg.threshold_game(games[g], int(p[g, k]), d)
+        with eg.ResidentGame(tg) as r:
+            _, pst = r.solve()
+            plain_ms += pst.solve_ms
+            plain_pairs += 1
+    plain = plain_pairs / K / (plain_ms / 1e3)
+    last = stats[-1]
+    b.free()
+    line = {"metric": "batched games/s (cfg4: 4096 uneven games x 8 mean-payoff thresholds, one launch)",
+            "value": value, "unit": "games/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int64",
+            "data": "synthetic",
+            "config": {"workload": "batched uneven games", "games": G, "thresholds": K, "d": d,
+                       "total_nodes": last.total_nodes, "total_edges": last.total_edges, "block": block,
+                       "graph_replayed": last.graph_replayed, "setup_s": setup_s},
+            "thresholds_per_s": value * K, "gteps": last.edges / (last.solve_ms * 1e6),
+            "plain": {"games_per_s": plain, "sample_pairs": plain_pairs,
+                      "how": "eg_dgame solve per (game, threshold), device time, seeded sample"},
+            "speedup_vs_plain": value / plain, "clocks": clocks,
+            "solve": {"rounds_max": last.rounds_max, "rounds_sum": last.rounds_sum, "lifts": last.lifts,
+                      "edges": last.edges, "num_top": last.num_top, "grid": last.grid}}
+    print(json.dumps(line), flush=True)
+
+
+def run_served(args):
+    """cfg5: Poisson arrivals of mean-payoff threshold queries against the
+    serving loop, rate swept; the plain reference point serves the same
+    arrivals one game at a time (FIFO, service time = measured plain solves)."""
+    import egsolver_b200 as eg
+    from egsolver_b200 import workloads
+
+    reqs = workloads.cfg5_requests(args.requests, n_max=args.n_max)
+    rng = np.random.default_rng(11)
+    # plain service time of every request: K single-game solves
+    plain_service = []
+    for g, p, d in reqs:
+        t = 0.0
+        with eg.ResidentGame(eg.threshold_game(g, int(p[0]), d)) as r:
+            _, st0 = r.solve()
+        for k in range(len(p)):
+            _, st = eg.solve(eg.threshold_game(g, int(p[k]), d))
+            t += st.solve_ms
+        plain_service.append(t)
+    results = []
+    for rate in [float(x) for x in args.rates.split(",")]:
+        arrivals = np.cumsum(rng.exponential(1.0 / rate, size=len(reqs)))
+        with eg.Server() as srv:
+            gids = [srv.add_game(g) for g, _, _ in reqs]
+            t0 = time.perf_counter()
+            qids = []
+            for i, (g, p, d) in enumerate(reqs):
+                delay = arrivals[i] - (time.perf_counter() - t0)
+                if delay > 0:
+                    time.sleep(delay)
+                qids.append(srv.submit(gids[i], p, d))
+            for q in qids:
+                srv.wait(q, 3_600_000)
+            st = srv.stats()
+        # the same arrivals served one game at a time
+        fin, lat = 0.0, []
+        for a, s in zip(arrivals, plain_service):
+            start = max(a, fin)
+            fin = start + s / 1e3
+            lat.append((fin - a) * 1e3)
+        solves = sum(len(p) for _, p, _ in reqs)
+        results.append({"rate": rate, "p50_ms": st["latency_p50_ms"], "p99_ms": st["latency_p99_ms"],
+                        "solves_per_s": st["solves_per_s"], "micro_batches": st["micro_batches"],
+                        "plain_p50_ms": float(np.percentile(lat, 50)), "plain_p99_ms": float(np.percentile(lat, 99)),
+                        "plain_solves_per_s": solves / fin})
+    best = max(results, key=lambda r: r["solves_per_s"])
+    line = {"metric": "served threshold solves/s with p50/p99 latency (cfg5, Poisson arrivals)",
+            "value": best["solves_per_s"], "unit": "solves/s", "n_gpus": 1, "steps": len(results), "warmup": 0,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int64", "data": "synthetic",
+            "config": {"workload": "served threshold queries", "requests": len(reqs), "n_max": args.n_max,
+                       "rates": args.rates},
+            "sweep": results}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         run_reference(args)
+        return
+    if args.workload == "cfg4":
+        run_batched(args)
+        return
+    if args.workload == "cfg5":
+        run_served(args)
         return
     import torch
 

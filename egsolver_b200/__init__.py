@@ -21,7 +21,7 @@ from . import _ffi
 from ._ffi import (EG_TOP32, EG_TOP64, VARIANT_AUTO, VARIANT_CTA, VARIANT_SMEM, VARIANT_THREAD,  # noqa: F401
                    VARIANT_WARP)
 
-__all__ = ["Game", "EGError", "Stats", "solve", "ResidentGame", "Batch", "BatchStats", "threshold_game",
+__all__ = ["Game", "EGError", "Stats", "solve", "ResidentGame", "Batch", "BatchStats", "Server", "threshold_game",
            "generate", "read_game", "read_game_text",
            "csr2csc", "compute_mg", "default_max_loop", "device_count", "CancelFlag", "EG_TOP32", "EG_TOP64",
            "lib"]
@@ -134,7 +134,7 @@ class Stats:
 
 def make_opts(credit_bits: int = 64, variant: int = VARIANT_AUTO, max_rounds: int = -1, timeout_ms: float = 0.0,
               device: int = 0, lanes_per_vertex: int = 0, small_max_deg: int = 0, large_min_deg: int = 0,
-              keep_layout: bool = False, cancel: Optional["CancelFlag"] = None) -> _ffi.EgOpts:
+              keep_layout: bool = False, cancel: Optional["CancelFlag"] = None, grid_ctas: int = 0) -> _ffi.EgOpts:
     o = _ffi.EgOpts()
     lib().eg_opts_default(C.byref(o))
     o.credit_bits = credit_bits
@@ -146,6 +146,7 @@ def make_opts(credit_bits: int = 64, variant: int = VARIANT_AUTO, max_rounds: in
     o.small_max_deg = small_max_deg
     o.large_min_deg = large_min_deg
     o.keep_layout = 1 if keep_layout else 0
+    o.grid_ctas = grid_ctas
     o.cancel = cancel.ptr if cancel is not None else None
     return o
 
@@ -342,6 +343,72 @@ class Batch:
 
     def __exit__(self, *exc):
         self.free()
+
+
+class Server:
+    """Serving loop for mean-payoff threshold queries (eg_serve_*): games are
+    registered once, queries are submitted at any time and run in
+    continuously formed micro-batches."""
+
+    def __init__(self, device: int = 0, max_inflight: int = 0, streams: int = 0, block: int = 0,
+                 hbm_reserve_bytes: int = 0, max_rounds: int = -1, large_ctas: int = 0):
+        o = _ffi.EgServeOpts()
+        o.device, o.max_inflight, o.streams, o.block = device, max_inflight, streams, block
+        o.hbm_reserve_bytes, o.max_rounds, o.large_ctas = hbm_reserve_bytes, max_rounds, large_ctas
+        self._h = C.c_void_p()
+        _check(lib().eg_serve_create(C.byref(o), C.byref(self._h)))
+        self._sizes: dict[int, int] = {}
+        self._qk: dict[int, tuple[int, int]] = {}
+
+    def add_game(self, game: Game) -> int:
+        gid = C.c_int64()
+        cg = game.c_struct()
+        _check(lib().eg_serve_add_game(self._h, C.byref(cg), C.byref(gid)))
+        self._sizes[gid.value] = game.num_nodes
+        return int(gid.value)
+
+    def remove_game(self, gid: int) -> None:
+        _check(lib().eg_serve_remove_game(self._h, gid))
+
+    def submit(self, gid: int, p, d: int = 1) -> int:
+        a = np.ascontiguousarray(p, dtype=np.int32).reshape(-1)
+        qid = C.c_int64()
+        _check(lib().eg_serve_submit(self._h, gid, a.ctypes.data, a.size, d, C.byref(qid)))
+        self._qk[qid.value] = (gid, a.size)
+        return int(qid.value)
+
+    def poll(self, qid: int) -> tuple[int, float]:
+        st = C.c_int32()
+        lat = C.c_double()
+        _check(lib().eg_serve_poll(self._h, qid, C.byref(st), C.byref(lat)))
+        return int(st.value), float(lat.value)
+
+    def wait(self, qid: int, timeout_ms: float = -1.0) -> None:
+        _check(lib().eg_serve_wait(self._h, qid, timeout_ms))
+
+    def result(self, qid: int) -> tuple[np.ndarray, int]:
+        gid, k = self._qk[qid]
+        out = np.zeros(k * self._sizes[gid], dtype=np.int64)
+        r = C.c_int64()
+        _check(lib().eg_serve_result(self._h, qid, out.ctypes.data, C.byref(r)))
+        del self._qk[qid]
+        return out.reshape(k, -1), int(r.value)
+
+    def stats(self) -> dict:
+        s = _ffi.EgServeStats()
+        _check(lib().eg_serve_stats_get(self._h, C.byref(s)))
+        return s.as_dict()
+
+    def close(self) -> None:
+        if self._h:
+            _check(lib().eg_serve_destroy(self._h))
+            self._h = C.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
 
 
 def threshold_game(game: Game, p: int, d: int) -> Game:

@@ -47,7 +47,8 @@ class EgOpts(C.Structure):
         ("device", C.c_int32),
         ("lanes_per_vertex", C.c_int32),
         ("keep_layout", C.c_int32),
-        ("reserved", C.c_int32 * 5),
+        ("grid_ctas", C.c_int32),
+        ("reserved", C.c_int32 * 4),
     ]
 
 
@@ -134,6 +135,33 @@ class EgBatchStats(C.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_ if k != "reserved"}
 
 
+class EgServeOpts(C.Structure):
+    _fields_ = [
+        ("device", C.c_int32),
+        ("max_inflight", C.c_int32),
+        ("streams", C.c_int32),
+        ("block", C.c_int32),
+        ("hbm_reserve_bytes", C.c_int64),
+        ("max_rounds", C.c_int64),
+        ("large_ctas", C.c_int32),
+        ("reserved", C.c_int32 * 5),
+    ]
+
+
+class EgServeStats(C.Structure):
+    _fields_ = [
+        ("submitted", C.c_int64), ("admitted", C.c_int64), ("completed", C.c_int64), ("failed", C.c_int64),
+        ("games_registered", C.c_int64), ("games_resident", C.c_int64), ("game_uploads", C.c_int64),
+        ("evictions", C.c_int64), ("micro_batches", C.c_int64), ("threshold_solves", C.c_int64),
+        ("latency_p50_ms", C.c_double), ("latency_p99_ms", C.c_double), ("latency_mean_ms", C.c_double),
+        ("latency_max_ms", C.c_double), ("elapsed_s", C.c_double), ("queries_per_s", C.c_double),
+        ("solves_per_s", C.c_double), ("device_bytes", C.c_int64), ("reserved", C.c_int32 * 6),
+    ]
+
+    def as_dict(self) -> dict:
+        return {k: getattr(self, k) for k, _ in self._fields_ if k != "reserved"}
+
+
 # every symbol the header declares, with (restype, argtypes)
 _P = C.c_void_p
 _I32, _I64 = C.c_int32, C.c_int64
@@ -172,6 +200,15 @@ SIGNATURES = {
     "eg_batch_tune": (_I32, [_P, C.POINTER(_I32)]),
     "eg_batch_device_bytes": (_I64, [_P]),
     "eg_batch_free": (None, [_P]),
+    "eg_serve_create": (_I32, [C.POINTER(EgServeOpts), C.POINTER(_P)]),
+    "eg_serve_add_game": (_I32, [_P, C.POINTER(EgGame), C.POINTER(_I64)]),
+    "eg_serve_remove_game": (_I32, [_P, _I64]),
+    "eg_serve_submit": (_I32, [_P, _I64, _P, _I32, _I32, C.POINTER(_I64)]),
+    "eg_serve_poll": (_I32, [_P, _I64, C.POINTER(_I32), C.POINTER(C.c_double)]),
+    "eg_serve_wait": (_I32, [_P, _I64, C.c_double]),
+    "eg_serve_result": (_I32, [_P, _I64, _P, C.POINTER(_I64)]),
+    "eg_serve_stats_get": (_I32, [_P, C.POINTER(EgServeStats)]),
+    "eg_serve_destroy": (_I32, [_P]),
 }
 
 _lib = None

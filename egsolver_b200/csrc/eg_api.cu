@@ -85,6 +85,12 @@ struct eg_dgame {
     void *d_F, *d_out;
     uint32_t *d_B;
     Ctrl *d_ctrl;
+    /* heavy vertices cut into edge tasks (AUTO layout) */
+    int4 *d_tasks;
+    void *d_hacc;
+    int *d_hrem, *d_toff;
+    long long task_cap;
+    int num_tasks, heavy_begin, heavy_bucket;
     size_t bytes;
     long long mg;
     int solved_bits;
@@ -188,7 +194,8 @@ extern "C" void eg_dgame_free(eg_dgame *g)
     if (g->st) cudaStreamSynchronize(g->st);
     void *ptrs[] = {g->d_rowptr, g->d_succ, g->d_w, g->d_owner, g->d_perm, g->d_iperm, g->d_P, g->d_CP,
                     g->d_CS, g->d_E, g->d_active0, g->d_k0, g->d_v0, g->d_k1, g->d_v1, g->d_scratch,
-                    g->d_counts, g->d_mg, g->d_F, g->d_out, g->d_B, g->d_ctrl};
+                    g->d_counts, g->d_mg, g->d_F, g->d_out, g->d_B, g->d_ctrl, g->d_tasks, g->d_hacc,
+                    g->d_hrem, g->d_toff};
     for (void *p : ptrs)
         if (p) cudaFree(p);
     for (int i = 0; i < 4; i++)
@@ -250,6 +257,11 @@ static eg_status dgame_alloc(const eg_game *game, const eg_opts *opts, eg_dgame 
     if (s == EG_OK) s = dalloc(g, (int64_t **)&g->d_out, (size_t)g->n);
     if (s == EG_OK) s = dalloc(g, &g->d_B, (size_t)(2 * words));
     if (s == EG_OK) s = dalloc(g, &g->d_ctrl, 1);
+    g->task_cap = g->m_pad_cap / (2 * kTaskPairs) + g->n_pad_cap + 2;
+    if (s == EG_OK) s = dalloc(g, &g->d_tasks, (size_t)g->task_cap);
+    if (s == EG_OK) s = dalloc(g, (int64_t **)&g->d_hacc, (size_t)g->n_pad_cap);
+    if (s == EG_OK) s = dalloc(g, &g->d_hrem, (size_t)g->n_pad_cap);
+    if (s == EG_OK) s = dalloc(g, &g->d_toff, (size_t)g->n_pad_cap + 1);
     if (s != EG_OK) {
         eg_dgame_free(g);
         return s;
@@ -367,6 +379,34 @@ static eg_status dgame_prepare(eg_dgame *g, const eg_opts *opts)
     radix_sort_pairs(g->d_k0, g->d_v0, g->d_k1, g->d_v1, g->m, bits_for(n_pad + 1), g->d_scratch, st, &sk, &sv);
     EG_CUDA(cudaMemcpyAsync(g->d_CS, sv, sizeof(int) * (size_t)g->m, cudaMemcpyDeviceToDevice, st));
     g->launches += 8 + 3 * ((bits_for(n_pad + 1) + 7) / 8) * 2;
+    /* AUTO layout: vertices of the warp / CTA buckets become 256-edge tasks */
+    g->num_tasks = 0;
+    g->heavy_bucket = g->bb.nb;
+    g->heavy_begin = n_pad;
+    if (!opts || opts->variant == EG_VARIANT_AUTO || opts->variant == EG_VARIANT_SMEM) {
+        for (int b = 0; b < g->bb.nb; b++)
+            if (g->groups[b] == 32 || g->groups[b] == EG_GROUP_CTA) {
+                g->heavy_bucket = b;
+                break;
+            }
+        if (g->heavy_bucket < g->bb.nb) {
+            g->heavy_begin = ct.start[2 * g->heavy_bucket];
+            const int nh = n_pad - g->heavy_begin;
+            if (nh > 0) {
+                k_task_count<<<grid_for(nh + 1, kPrepBlock), kPrepBlock, 0, st>>>(g->heavy_begin, n_pad, g->d_P, kTaskPairs,
+                                                                                   g->d_toff);
+                excl_scan(g->d_toff, (long long)nh + 1, g->d_scratch, st);
+                int total = 0;
+                EG_CUDA(cudaMemcpyAsync(&total, g->d_toff + nh, sizeof total, cudaMemcpyDeviceToHost, st));
+                EG_CUDA(cudaStreamSynchronize(st));
+                if (total > g->task_cap) return eg_set_error(EG_ERR_INVALID, "task list overflow (%d tasks)", total);
+                k_task_fill<<<grid_for(nh, kPrepBlock), kPrepBlock, 0, st>>>(g->heavy_begin, n_pad, g->d_P, kTaskPairs,
+                                                                               g->d_toff, ct, g->d_tasks);
+                g->num_tasks = total;
+                g->launches += 5;
+            }
+        }
+    }
     EG_CUDA(cudaGetLastError());
     g->prepared = true;
     return EG_OK;
@@ -418,8 +458,14 @@ extern "C" eg_status eg_dgame_solve(eg_dgame *g, const eg_opts *opts_in, eg_stat
         p.cancel = (const int *)dp;
     }
     p.n_pad = n_pad;
+    const bool small = n_pad <= kSmallGameMaxPad &&
+                       (opts->variant == EG_VARIANT_SMEM || (opts->variant == EG_VARIANT_AUTO && g->m <= kSmallGameEdges));
+    /* the grid kernel lifts heavy buckets as tasks; the one-CTA kernel
+     * lifts every class by words */
+    const bool tasks = !small && g->num_tasks > 0;
     int nc = 0;
     for (int b = g->bb.nb - 1; b >= 0; b--) {
+        if (tasks && b >= g->heavy_bucket) continue;
         for (int own = 0; own < 2; own++) {
             const int c = b * 2 + own;
             if (g->ct.count[c] == 0) continue;
@@ -432,16 +478,23 @@ extern "C" eg_status eg_dgame_solve(eg_dgame *g, const eg_opts *opts_in, eg_stat
         }
     }
     p.nclasses = nc;
+    if (tasks) {
+        launch_task_reset(bits, g->heavy_begin, n_pad, g->d_toff, g->ct, g->d_hacc, g->d_hrem, st);
+        g->launches++;
+        p.tasks = g->d_tasks;
+        p.num_tasks = g->num_tasks;
+        p.heavy_begin = g->heavy_begin;
+        p.hacc = g->d_hacc;
+        p.hrem = g->d_hrem;
+    }
     int grid = 0, block = 0;
-    const bool small = n_pad <= kSmallGameMaxPad &&
-                       (opts->variant == EG_VARIANT_SMEM || (opts->variant == EG_VARIANT_AUTO && g->m <= kSmallGameEdges));
     EG_CUDA(cudaEventRecord(g->ev[1], st));
     if (small) {
         EG_TRY(launch_lift_cta(p, bits, st));
         grid = 1;
         block = 1024;
     } else {
-        EG_TRY(launch_lift(p, bits, st, &grid, &block));
+        EG_TRY(launch_lift(p, bits, st, &grid, &block, opts->grid_ctas));
     }
     g->launches++;
     EG_CUDA(cudaEventRecord(g->ev[2], st));

@@ -18,7 +18,7 @@
  * weights w * d - p_k.  No wait in this kernel spins: rounds end at
  * __syncthreads and games come from an atomic counter.
  */
-#include "eg_prep.cuh"
+#include "eg_batch.cuh"
 
 #include <algorithm>
 #include <cstdio>
@@ -43,35 +43,6 @@ using namespace eg;
     } while (0)
 
 namespace {
-
-constexpr int kMaxGameNodes = 1 << 19;
-
-struct BatchCtrl {
-    int next_game;
-    int pad;
-    unsigned long long lifts, edges, num_top;
-    unsigned long long t_start;
-};
-
-struct BatchParams {
-    const long long *node_off;   /* num_games + 1                       */
-    const int *order;            /* game queue order (largest first)    */
-    const int *P;                /* global edge offsets, total_nodes+1  */
-    const int2 *E;               /* {global successor, weight}          */
-    const int *CP;               /* CSC offsets                         */
-    const int *CS;               /* CSC predecessors (global ids)       */
-    const unsigned char *owner;
-    const int *minw, *maxw;      /* per vertex                          */
-    const int *thr;              /* p[g * K + k]                        */
-    long long *F;                /* credits [v * K + k]                 */
-    long long *rounds;           /* per game                            */
-    int *status;                 /* per game                            */
-    BatchCtrl *ctrl;
-    int num_games, K, d;
-    int words_max;               /* shared bitmap words per buffer      */
-    long long max_rounds;
-    unsigned long long timeout_ns;
-};
 
 __device__ __forceinline__ int nth_bit(uint32_t w, int k)
 {
@@ -111,8 +82,6 @@ __global__ void __launch_bounds__(1024) k_batch_solve(const __grid_constant__ Ba
     const int tid = threadIdx.x, lane = tid & 31;
     const int grp = lane / KP, gl = lane % KP;
     const unsigned gmask = (KP == 32) ? 0xffffffffu : (((1u << KP) - 1u) << (grp * KP));
-    const int K = p.K;
-    const long long d = p.d;
     const long long TOP = (long long)INT64_MAX;
     unsigned long long lifts = 0, edges = 0, ntop = 0;
     if (blockIdx.x == 0 && tid == 0) p.ctrl->t_start = globaltimer_ns();
@@ -121,13 +90,19 @@ __global__ void __launch_bounds__(1024) k_batch_solve(const __grid_constant__ Ba
         __syncthreads();
         const int gi = s_game;
         if (gi >= p.num_games) break;
-        const int g = p.order[gi];
-        const long long base = p.node_off[g];
-        const int n = (int)(p.node_off[g + 1] - base);
+        const GameDesc gd = p.games[p.order ? p.order[gi] : gi];
+        const long long base = gd.base;
+        const int n = gd.n;
+        const int K = gd.K;
+        const long long d = gd.d;
+        const int *P = gd.P;
+        const int2 *E = gd.E;
+        const unsigned char *owner = gd.owner;
+        long long *F = gd.F - base * K; /* indexed by id * K + k with ids base-relative */
         const int W = (n + 31) >> 5;
         uint32_t *cur = sm, *nxt = sm + p.words_max;
         if (tid < KP) {
-            s_p[tid] = p.thr[(long long)g * K + (tid < K ? tid : 0)];
+            s_p[tid] = gd.thr[tid < K ? tid : 0];
             s_mg[tid] = 0;
         }
         if (tid < 2) s_ctr[tid] = 0;
@@ -139,9 +114,9 @@ __global__ void __launch_bounds__(1024) k_batch_solve(const __grid_constant__ Ba
         /* f = 0, MG per threshold, initial frontier (any threshold) */
         for (int v = tid; v < n; v += blockDim.x) {
             const long long gv = base + v;
-            for (int k = 0; k < K; k++) p.F[gv * K + k] = 0;
-            const long long lo = (long long)p.minw[gv] * d, hi = (long long)p.maxw[gv] * d;
-            const int own = p.owner[gv];
+            for (int k = 0; k < K; k++) F[gv * K + k] = 0;
+            const long long lo = (long long)gd.minw[v] * d, hi = (long long)gd.maxw[v] * d;
+            const int own = owner[v];
             bool act = false;
             for (int k = 0; k < K; k++) act |= own ? (lo - s_p[k] < 0) : (hi - s_p[k] < 0);
             if (act) atomicOr(&cur[v >> 5], 1u << (v & 31));
@@ -149,7 +124,7 @@ __global__ void __launch_bounds__(1024) k_batch_solve(const __grid_constant__ Ba
         for (int k = 0; k < K; k++) {
             long long s = 0;
             for (int v = tid; v < n; v += blockDim.x) {
-                const long long x = (long long)s_p[k] - (long long)p.minw[base + v] * d;
+                const long long x = (long long)s_p[k] - (long long)gd.minw[v] * d;
                 s += x > 0 ? x : 0;
             }
 #pragma unroll
@@ -178,29 +153,29 @@ __global__ void __launch_bounds__(1024) k_batch_solve(const __grid_constant__ Ba
                     if (grp < c) {
                         const int v = (w0 << 5) + nth_bit(word, grp);
                         const long long gv = base + v;
-                        const int own = p.owner[gv];
+                        const int own = owner[v];
                         long long acc = own ? 0 : TOP;
-                        const int eb = p.P[gv], ee = p.P[gv + 1];
+                        const int eb = P[v], ee = P[v + 1];
                         for (int e = eb; e < ee; e++) {
-                            const int2 q = __ldg(p.E + e);
+                            const int2 q = __ldg(E + e);
                             if (valid) {
-                                const long long val = ominus64(p.F[(long long)q.x * K + gl], (long long)q.y * d - pk, mgk);
+                                const long long val = ominus64(F[(long long)q.x * K + gl], (long long)q.y * d - pk, mgk);
                                 acc = own ? (val > acc ? val : acc) : (val < acc ? val : acc);
                             }
                         }
                         bool ch = false;
                         if (valid) {
-                            const long long old = p.F[gv * K + gl];
+                            const long long old = F[gv * K + gl];
                             if (old < acc) {
-                                p.F[gv * K + gl] = acc;
+                                F[gv * K + gl] = acc;
                                 ch = true;
                             }
                         }
                         const unsigned chm = __ballot_sync(gmask, ch) & gmask;
                         if (chm) {
-                            const int cb = p.CP[gv], ce = p.CP[gv + 1];
+                            const int cb = gd.CP[v], ce = gd.CP[v + 1];
                             for (int j = cb + gl; j < ce; j += KP) {
-                                const int pr = (int)(p.CS[j] - base);
+                                const int pr = (int)(gd.CS[j] - base);
                                 const uint32_t bit = 1u << (pr & 31);
                                 if (!(atomicOr(&nxt[pr >> 5], bit) & bit)) any_new = 1;
                             }
@@ -236,10 +211,10 @@ __global__ void __launch_bounds__(1024) k_batch_solve(const __grid_constant__ Ba
             nxt = t;
         }
         /* TOP count of this game (all thresholds) */
-        for (long long i = tid; i < (long long)n * K; i += blockDim.x) ntop += (p.F[base * K + i] == TOP);
+        for (long long i = tid; i < (long long)n * K; i += blockDim.x) ntop += (gd.F[i] == TOP);
         if (tid == 0) {
-            p.rounds[g] = r;
-            p.status[g] = st;
+            *gd.rounds = r;
+            *gd.status = st;
         }
         __syncthreads();
     }
@@ -255,6 +230,10 @@ __global__ void __launch_bounds__(1024) k_batch_solve(const __grid_constant__ Ba
         atomicAdd(&p.ctrl->num_top, ntop);
     }
 }
+
+}  // namespace
+
+namespace eg {
 
 /* one warp per vertex of the packed graph: CSC sort input and in-degrees */
 __global__ void k_batch_expand(long long total_nodes, const int *P, const int2 *E, int *key, int *val, int *indeg)
@@ -272,6 +251,133 @@ __global__ void k_batch_expand(long long total_nodes, const int *P, const int2 *
     }
 }
 
+size_t layout_bytes(int n, long long m)
+{
+    return sizeof(int) * ((size_t)n + 1) * 2 + sizeof(int) * (size_t)m + sizeof(int2) * (size_t)m + (size_t)n +
+           2 * sizeof(int) * (size_t)n + 4096;
+}
+
+size_t layout_build_bytes(int n, long long m)
+{
+    return sizeof(int) * 4 * (size_t)(m + 1) + sizeof(int) * (size_t)(radix_scratch_ints(m) + scan_scratch_ints(n + 1) + 64);
+}
+
+void layout_free(GameLayout *l, cudaStream_t st)
+{
+    void *ptrs[] = {l->P, l->CP, l->CS, l->minw, l->maxw, l->E, l->owner};
+    for (void *q : ptrs)
+        if (q) cudaFreeAsync(q, st);
+    memset(l, 0, sizeof *l);
+}
+
+eg_status layout_upload(const eg_game &G, cudaStream_t st, GameLayout *out)
+{
+    GameLayout L;
+    memset(&L, 0, sizeof L);
+    const int n = G.num_nodes;
+    const long long m = G.num_edges;
+    L.n = n;
+    L.m = m;
+    std::vector<int> P((size_t)n + 1), minw((size_t)n), maxw((size_t)n);
+    std::vector<int2> E((size_t)m);
+    std::vector<unsigned char> own((size_t)n);
+    for (int v = 0; v < n; v++) {
+        P[(size_t)v] = (int)G.row_ptr[v];
+        own[(size_t)v] = G.owner ? G.owner[v] : (unsigned char)(v >= G.num_nodes0);
+        int mn = INT32_MAX, mx = INT32_MIN;
+        for (long long j = G.row_ptr[v]; j < G.row_ptr[v + 1]; j++) {
+            E[(size_t)j] = make_int2(G.succ[j], G.weight[j]);
+            mn = std::min(mn, G.weight[j]);
+            mx = std::max(mx, G.weight[j]);
+        }
+        minw[(size_t)v] = mn;
+        maxw[(size_t)v] = mx;
+    }
+    P[(size_t)n] = (int)m;
+    cudaError_t e = cudaSuccess;
+    /* stream-ordered allocations: no device-wide synchronisation, so kernels
+     * already running on other streams keep running during an upload */
+#define LA(ptr, cnt)                                                         \
+    if (e == cudaSuccess) {                                                  \
+        e = cudaMallocAsync((void **)&ptr, std::max<size_t>(sizeof(*ptr) * (size_t)(cnt), 16), st); \
+    }
+    LA(L.P, n + 1);
+    LA(L.CP, n + 1);
+    LA(L.CS, m);
+    LA(L.E, m);
+    LA(L.owner, n);
+    LA(L.minw, n);
+    LA(L.maxw, n);
+    int *k0 = nullptr, *v0 = nullptr, *k1 = nullptr, *v1 = nullptr, *scr = nullptr;
+    LA(k0, m + 1);
+    LA(v0, m + 1);
+    LA(k1, m + 1);
+    LA(v1, m + 1);
+    LA(scr, radix_scratch_ints(m) + scan_scratch_ints((long long)n + 1) + 64);
+#undef LA
+    if (e == cudaSuccess) e = cudaMemcpyAsync(L.P, P.data(), sizeof(int) * ((size_t)n + 1), cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(L.E, E.data(), sizeof(int2) * (size_t)m, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(L.owner, own.data(), (size_t)n, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(L.minw, minw.data(), sizeof(int) * (size_t)n, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(L.maxw, maxw.data(), sizeof(int) * (size_t)n, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) e = cudaMemsetAsync(L.CP, 0, sizeof(int) * ((size_t)n + 1), st);
+    if (e == cudaSuccess) {
+        long long gr = ((long long)n * 32 + 255) / 256;
+        if (gr > 148 * 32) gr = 148 * 32;
+        k_batch_expand<<<(unsigned)gr, 256, 0, st>>>(n, L.P, L.E, k0, v0, L.CP);
+        excl_scan(L.CP, (long long)n + 1, scr, st);
+        int *sk, *sv;
+        radix_sort_pairs(k0, v0, k1, v1, m, bits_for(n), scr, st, &sk, &sv);
+        e = cudaMemcpyAsync(L.CS, sv, sizeof(int) * (size_t)m, cudaMemcpyDeviceToDevice, st);
+    }
+    if (k0) cudaFreeAsync(k0, st);
+    if (v0) cudaFreeAsync(v0, st);
+    if (k1) cudaFreeAsync(k1, st);
+    if (v1) cudaFreeAsync(v1, st);
+    if (scr) cudaFreeAsync(scr, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        layout_free(&L, st);
+        cudaStreamSynchronize(st);
+        return eg_set_error(e == cudaErrorMemoryAllocation ? EG_ERR_OOM : EG_ERR_CUDA, "game upload failed: %s",
+                            cudaGetErrorString(e));
+    }
+    L.bytes = layout_bytes(n, m);
+    *out = L;
+    return EG_OK;
+}
+
+GameDesc layout_desc(const GameLayout &l, const int *thr, long long *F, long long *rounds, int *status, int K, int d)
+{
+    GameDesc D;
+    memset(&D, 0, sizeof D);
+    D.P = l.P;
+    D.E = l.E;
+    D.CP = l.CP;
+    D.CS = l.CS;
+    D.owner = l.owner;
+    D.minw = l.minw;
+    D.maxw = l.maxw;
+    D.thr = thr;
+    D.F = F;
+    D.rounds = rounds;
+    D.status = status;
+    D.base = 0;
+    D.n = l.n;
+    D.K = K;
+    D.d = d;
+    return D;
+}
+
+}  // namespace eg
+
+namespace {
+
+}  // namespace
+
+namespace eg {
+
 typedef void (*batch_kernel_t)(BatchParams);
 
 batch_kernel_t kernel_for(int kp)
@@ -285,6 +391,32 @@ batch_kernel_t kernel_for(int kp)
     default: return k_batch_solve<32>;
     }
 }
+
+eg_status launch_batch(const BatchParams &p, int KP, int block, int num_sms, cudaStream_t st, int *grid_out)
+{
+    batch_kernel_t fn = kernel_for(KP);
+    const size_t smem = sizeof(uint32_t) * 2 * (size_t)p.words_max;
+    cudaError_t e = cudaFuncSetAttribute((const void *)fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return eg_set_error(EG_ERR_CUDA, "shared memory request failed: %s", cudaGetErrorString(e));
+    int per_sm = 0;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void *)fn, block, smem);
+    if (e != cudaSuccess || per_sm < 1)
+        return eg_set_error(EG_ERR_CUDA, "batch kernel does not fit (block %d, %zu B shared)", block, smem);
+    int grid = num_sms * per_sm;
+    if (grid > p.num_games) grid = p.num_games;
+    if (grid < 1) grid = 1;
+    e = cudaMemsetAsync(p.ctrl, 0, sizeof(BatchCtrl), st);
+    if (e != cudaSuccess) return eg_set_error(EG_ERR_CUDA, "cudaMemsetAsync failed: %s", cudaGetErrorString(e));
+    void *args[] = {(void *)&p};
+    e = cudaLaunchKernel((const void *)fn, dim3(grid), dim3(block), args, smem, st);
+    if (e != cudaSuccess) return eg_set_error(EG_ERR_CUDA, "batch kernel launch failed: %s", cudaGetErrorString(e));
+    *grid_out = grid;
+    return EG_OK;
+}
+
+}  // namespace eg
+
+namespace {
 
 int pow2_at_least(int k)
 {
@@ -312,6 +444,7 @@ struct eg_batch {
     unsigned char *owner;
     long long *F, *rounds;
     BatchCtrl *ctrl;
+    GameDesc *desc;
     size_t bytes;
     bool thresholds_set, solved;
     bool use_graph;
@@ -342,7 +475,7 @@ extern "C" void eg_batch_free(eg_batch *b)
     if (b->graph_exec) cudaGraphExecDestroy(b->graph_exec);
     if (b->graph) cudaGraphDestroy(b->graph);
     void *ptrs[] = {b->node_off, b->order, b->P, b->CP, b->CS, b->minw, b->maxw, b->thr,
-                    b->status, b->E, b->owner, b->F, b->rounds, b->ctrl};
+                    b->status, b->E, b->owner, b->F, b->rounds, b->ctrl, b->desc};
     for (void *q : ptrs)
         if (q) cudaFree(q);
     if (b->ev0) cudaEventDestroy(b->ev0);
@@ -366,9 +499,9 @@ extern "C" eg_status eg_batch_create(const eg_game *games, int32_t num_games, co
     for (int g = 0; g < num_games; g++) {
         eg_status s = eg_validate(&games[g]);
         if (s != EG_OK) return eg_set_error(s, "game %d: %s", g, eg_last_error());
-        if (games[g].num_nodes > kMaxGameNodes)
+        if (games[g].num_nodes > kBatchMaxGameNodes)
             return eg_set_error(EG_ERR_INVALID, "game %d has %d vertices; the batch path holds at most %d per game",
-                                g, games[g].num_nodes, kMaxGameNodes);
+                                g, games[g].num_nodes, kBatchMaxGameNodes);
         tn += games[g].num_nodes;
         tm += games[g].num_edges;
         nmax = std::max(nmax, games[g].num_nodes);
@@ -444,14 +577,38 @@ extern "C" eg_status eg_batch_create(const eg_game *games, int32_t num_games, co
     if (s == EG_OK) s = balloc(b, &b->rounds, (size_t)num_games);
     if (s == EG_OK) s = balloc(b, &b->status, (size_t)num_games);
     if (s == EG_OK) s = balloc(b, &b->ctrl, 1);
+    if (s == EG_OK) s = balloc(b, &b->desc, (size_t)num_games);
     if (s != EG_OK) {
         eg_batch_free(b);
         return s;
+    }
+    /* one descriptor per game, pointing into the packed arrays */
+    std::vector<GameDesc> desc((size_t)num_games);
+    for (int g = 0; g < num_games; g++) {
+        const long long base = b->node_off_h[g];
+        GameDesc &D = desc[(size_t)g];
+        D.P = b->P + base;
+        D.E = b->E;
+        D.CP = b->CP + base;
+        D.CS = b->CS;
+        D.owner = b->owner + base;
+        D.minw = b->minw + base;
+        D.maxw = b->maxw + base;
+        D.thr = b->thr + (long long)g * b->K;
+        D.F = b->F + base * b->K;
+        D.rounds = b->rounds + g;
+        D.status = b->status + g;
+        D.base = base;
+        D.n = games[g].num_nodes;
+        D.K = b->K;
+        D.d = b->d;
+        D.pad = 0;
     }
     cudaStream_t st = b->st;
     e = cudaMemcpyAsync(b->node_off, b->node_off_h.data(), sizeof(long long) * ((size_t)num_games + 1),
                         cudaMemcpyHostToDevice, st);
     if (e == cudaSuccess) e = cudaMemcpyAsync(b->order, order.data(), sizeof(int) * (size_t)num_games, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(b->desc, desc.data(), sizeof(GameDesc) * desc.size(), cudaMemcpyHostToDevice, st);
     if (e == cudaSuccess) e = cudaMemcpyAsync(b->P, P.data(), sizeof(int) * ((size_t)tn + 1), cudaMemcpyHostToDevice, st);
     if (e == cudaSuccess) e = cudaMemcpyAsync(b->E, E.data(), sizeof(int2) * (size_t)tm, cudaMemcpyHostToDevice, st);
     if (e == cudaSuccess) e = cudaMemcpyAsync(b->owner, own.data(), (size_t)tn, cudaMemcpyHostToDevice, st);
@@ -505,23 +662,10 @@ extern "C" eg_status eg_batch_set_thresholds(eg_batch *b, const int32_t *p)
 static eg_status batch_params(eg_batch *b, BatchParams *p)
 {
     memset(p, 0, sizeof *p);
-    p->node_off = b->node_off;
+    p->games = b->desc;
     p->order = b->order;
-    p->P = b->P;
-    p->E = b->E;
-    p->CP = b->CP;
-    p->CS = b->CS;
-    p->owner = b->owner;
-    p->minw = b->minw;
-    p->maxw = b->maxw;
-    p->thr = b->thr;
-    p->F = b->F;
-    p->rounds = b->rounds;
-    p->status = b->status;
     p->ctrl = b->ctrl;
     p->num_games = b->num_games;
-    p->K = b->K;
-    p->d = b->d;
     p->words_max = b->words_max;
     p->max_rounds = b->max_rounds;
     p->timeout_ns = b->timeout_ms > 0 ? (unsigned long long)(b->timeout_ms * 1e6) : 0ull;
@@ -533,23 +677,9 @@ static eg_status batch_enqueue(eg_batch *b, int block, int *grid_out)
 {
     BatchParams p;
     batch_params(b, &p);
-    batch_kernel_t fn = kernel_for(b->KP);
-    const size_t smem = sizeof(uint32_t) * 2 * (size_t)b->words_max;
-    cudaError_t e = cudaFuncSetAttribute((const void *)fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e != cudaSuccess) return eg_set_error(EG_ERR_CUDA, "shared memory request failed: %s", cudaGetErrorString(e));
-    int per_sm = 0;
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void *)fn, block, smem);
-    if (e != cudaSuccess || per_sm < 1)
-        return eg_set_error(EG_ERR_CUDA, "batch kernel does not fit (block %d, %zu B shared)", block, smem);
     int sms = 0;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, b->device);
-    int grid = sms * per_sm;
-    if (grid > b->num_games) grid = b->num_games;
-    EG_CUDA(cudaMemsetAsync(b->ctrl, 0, sizeof(BatchCtrl), b->st));
-    void *args[] = {(void *)&p};
-    EG_CUDA(cudaLaunchKernel((const void *)fn, dim3(grid), dim3(block), args, smem, b->st));
-    *grid_out = grid;
-    return EG_OK;
+    return launch_batch(p, b->KP, block, sms, b->st, grid_out);
 }
 
 extern "C" eg_status eg_batch_solve(eg_batch *b, eg_batch_stats *stats)

@@ -207,9 +207,11 @@ __device__ __noinline__ void thread_class(const LiftParams &p, const LiftClass &
     const int gwarp = (int)((blockIdx.x * (unsigned)blockDim.x + threadIdx.x) >> 5);
     const int nwarp = (int)((gridDim.x * (unsigned)blockDim.x) >> 5);
     const int nwords = lc.word_end - lc.word_begin;
-    for (int w0 = gwarp * U; w0 < nwords; w0 += nwarp * U) {
+    /* every warp gets the same number of words (+-1) of this class */
+    const int lo = (int)((long long)gwarp * nwords / nwarp), hi = (int)((long long)(gwarp + 1) * nwords / nwarp);
+    for (int w0 = lo; w0 < hi; w0 += U) {
         uint32_t mine = 0;
-        if (lane < U && w0 + lane < nwords) {
+        if (lane < U && w0 + lane < hi) {
             uint32_t *wp = cur + lc.word_begin + w0 + lane;
             mine = __ldcg(wp);
             if (mine) __stcg(wp, 0u);
@@ -261,6 +263,113 @@ __device__ __noinline__ void thread_class(const LiftParams &p, const LiftClass &
                 }
             }
         }
+    }
+}
+
+template <int OWNER>
+__device__ __forceinline__ void atomic_combine(int32_t *a, int32_t v)
+{
+    if (OWNER) atomicMax(a, v);
+    else atomicMin(a, v);
+}
+template <int OWNER>
+__device__ __forceinline__ void atomic_combine(int64_t *a, int64_t v)
+{
+    if (OWNER) atomicMax((long long *)a, (long long)v);
+    else atomicMin((long long *)a, (long long)v);
+}
+__device__ __forceinline__ int32_t atomic_swap(int32_t *a, int32_t v) { return atomicExch(a, v); }
+__device__ __forceinline__ int64_t atomic_swap(int64_t *a, int64_t v)
+{
+    return (int64_t)atomicExch((unsigned long long *)a, (unsigned long long)v);
+}
+
+/* The last step of a heavy vertex's lift (one warp): compare with the old
+ * credit, raise it, clear the vertex's frontier bit, push predecessors. */
+template <class T>
+__device__ __forceinline__ void heavy_finalize(const LiftParams &p, T *F, uint32_t *cur, uint32_t *nxt, int u, T v,
+                                               int lane, LiftCounters &cnt)
+{
+    int raise = 0;
+    if (lane == 0) {
+        const T old = ld_credit(F + u);
+        raise = old < v;
+        if (raise) {
+            st_credit(F + u, v);
+            cnt.changes++;
+        }
+        atomicAnd(cur + (u >> 5), ~(1u << (u & 31)));
+        cnt.lifts++;
+    }
+    raise = __shfl_sync(0xffffffffu, raise, 0);
+    if (raise) {
+        const int cb = __ldg(p.CP + u), ce = __ldg(p.CP + u + 1);
+        if (lane == 0) cnt.pushes += (unsigned)(ce - cb);
+        cnt.any_new |= ce > cb;
+        for (int k = cb + lane; k < ce; k += 32) bitmap_mark(nxt, __ldg(p.CS + k));
+    }
+}
+
+/* One task of a heavy vertex: up to kTaskPairs edge pairs, a warp-wide
+ * min/max; a vertex cut into several tasks combines the partial results
+ * with an atomic min/max, and the task that reports last finalizes. */
+template <class T, int OWNER>
+__device__ __forceinline__ void heavy_task(const LiftParams &p, T *F, uint32_t *cur, uint32_t *nxt, const int4 tk,
+                                           int lane, LiftCounters &cnt)
+{
+    T acc = identity<OWNER, T>();
+    int real = 0;
+#pragma unroll 4
+    for (int k = tk.y + lane; k < tk.z; k += 32) {
+        const int4 q = __ldg(p.E4 + k);
+        const T v0 = ominus<T>(ld_credit(F + q.x), q.y, p.mg);
+        const T v1 = ominus<T>(ld_credit(F + q.z), q.w, p.mg);
+        acc = combine<OWNER>(acc, combine<OWNER>(v0, v1));
+        real += 1 + (q.z < p.n_pad);
+    }
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) acc = combine<OWNER>(acc, shfl_xor<T>(0xffffffffu, acc, off, 32));
+    cnt.edges += (unsigned long long)real;
+    const int u = tk.x, nt = tk.w >> 1;
+    if (nt == 1) {
+        heavy_finalize<T>(p, F, cur, nxt, u, acc, lane, cnt);
+        return;
+    }
+    const int h = u - p.heavy_begin;
+    T *hacc = (T *)p.hacc;
+    int last = 0;
+    if (lane == 0) {
+        atomic_combine<OWNER>(hacc + h, acc);
+        __threadfence();
+        last = atomicSub(p.hrem + h, 1) == 1;
+    }
+    last = __shfl_sync(0xffffffffu, last, 0);
+    if (!last) return;
+    T v = (T)0;
+    if (lane == 0) {
+        __threadfence();
+        v = atomic_swap(hacc + h, identity<OWNER, T>());
+        p.hrem[h] = nt; /* ready for the next round */
+    }
+    v = shfl_idx<T>(0xffffffffu, v, 0, 32);
+    heavy_finalize<T>(p, F, cur, nxt, u, v, lane, cnt);
+}
+
+/* Heavy vertices: their edge tasks are dealt round-robin to all warps of
+ * the grid (balanced without any counter); a task of an inactive vertex
+ * costs one bitmap read. */
+template <class T>
+__device__ __noinline__ void heavy_tasks(const LiftParams &p, T *F, uint32_t *cur, uint32_t *nxt, LiftCounters &cnt)
+{
+    const int lane = threadIdx.x & 31;
+    const int gwarp = (int)((blockIdx.x * (unsigned)blockDim.x + threadIdx.x) >> 5);
+    const int nwarp = (int)((gridDim.x * (unsigned)blockDim.x) >> 5);
+    for (int t = gwarp; t < p.num_tasks; t += nwarp) {
+        const int4 tk = __ldg(p.tasks + t);
+        const uint32_t w = __ldcg(cur + (tk.x >> 5));
+        if (!((w >> (tk.x & 31)) & 1u)) continue;
+        if (tk.w & 1) heavy_task<T, 1>(p, F, cur, nxt, tk, lane, cnt);
+        else heavy_task<T, 0>(p, F, cur, nxt, tk, lane, cnt);
     }
 }
 
@@ -366,6 +475,7 @@ __global__ void __launch_bounds__(LIFT_BLOCK, 2) k_lift(const __grid_constant__ 
         uint32_t *nxt = (round & 1) ? p.B0 : p.B1;
         int *ctr = c->ctr[round & 1];
         cnt.any_new = 0;
+        if (p.num_tasks) heavy_tasks<T>(p, F, cur, nxt, cnt);
         for (int ci = 0; ci < p.nclasses; ci++) {
             const LiftClass &lc = p.cls[ci];
             if (lc.owner) run_class<T, 1>(p, lc, F, cur, nxt, ctr + ci, cnt);
@@ -540,7 +650,7 @@ eg_status launch_lift_cta(const LiftParams &p, int credit_bits, cudaStream_t st)
     return EG_OK;
 }
 
-eg_status launch_lift(const LiftParams &p, int credit_bits, cudaStream_t st, int *grid, int *block)
+eg_status launch_lift(const LiftParams &p, int credit_bits, cudaStream_t st, int *grid, int *block, int max_ctas)
 {
     int dev = 0;
     cudaGetDevice(&dev);
@@ -552,7 +662,8 @@ eg_status launch_lift(const LiftParams &p, int credit_bits, cudaStream_t st, int
     if (err != cudaSuccess || per_sm < 1)
         return eg_set_error(EG_ERR_CUDA, "occupancy query for the lifting kernel failed: %s",
                             cudaGetErrorString(err));
-    const int g = sms * per_sm;
+    int g = sms * per_sm;
+    if (max_ctas > 0 && max_ctas < g) g = max_ctas;
     void *args[] = {(void *)&p};
     err = cudaLaunchCooperativeKernel(fn, dim3(g), dim3(LIFT_BLOCK), args, 0, st);
     if (err != cudaSuccess)

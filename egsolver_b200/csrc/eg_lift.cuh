@@ -35,11 +35,20 @@ struct LiftParams {
     int n_pad;                 /* ids >= n_pad are the padding sentinels    */
     int nclasses;
     LiftClass cls[EG_MAX_CLASSES];
+    /* heavy vertices (ids >= heavy_begin) cut into edge tasks */
+    const int4 *tasks;         /* {vertex, first pair, end pair, (ntasks << 1) | owner } */
+    int num_tasks;
+    int heavy_begin;
+    void *hacc;                /* per heavy vertex: partial min / max (credit type) */
+    int *hrem;                 /* per heavy vertex: tasks still to report          */
 };
+
+/* Edge pairs per heavy task (256 edges). */
+constexpr int kTaskPairs = 128;
 
 /* Cooperative launch of the persistent lifting kernel on `st`; *grid gets
  * the number of CTAs used. */
-eg_status launch_lift(const LiftParams &p, int credit_bits, cudaStream_t st, int *grid, int *block);
+eg_status launch_lift(const LiftParams &p, int credit_bits, cudaStream_t st, int *grid, int *block, int max_ctas);
 /* One-CTA launch for small games (frontier in shared memory). */
 eg_status launch_lift_cta(const LiftParams &p, int credit_bits, cudaStream_t st);
 

@@ -354,6 +354,63 @@ __global__ void k_init_frontier(int n_pad, const int *perm, const unsigned char 
     }
 }
 
+/* ------------------------------------------------------------------ */
+/* Heavy vertices cut into edge tasks                                   */
+/* ------------------------------------------------------------------ */
+
+__global__ void k_task_count(int heavy_begin, int n_pad, const int *P, int task_pairs, int *count)
+{
+    const int nh = n_pad - heavy_begin;
+    for (long long h = (long long)blockIdx.x * blockDim.x + threadIdx.x; h <= nh; h += (long long)gridDim.x * blockDim.x) {
+        int c = 0;
+        if (h < nh) {
+            const int u = heavy_begin + (int)h;
+            const int pairs = (P[u + 1] - P[u]) >> 1;
+            c = (pairs + task_pairs - 1) / task_pairs;
+        }
+        count[h] = c;
+    }
+}
+
+__global__ void k_task_fill(int heavy_begin, int n_pad, const int *P, int task_pairs, const int *toff, ClassTable ct,
+                            int4 *tasks)
+{
+    const int nh = n_pad - heavy_begin;
+    for (long long h = (long long)blockIdx.x * blockDim.x + threadIdx.x; h < nh; h += (long long)gridDim.x * blockDim.x) {
+        const int u = heavy_begin + (int)h;
+        const int b = P[u] >> 1, e = P[u + 1] >> 1;
+        const int nt = toff[h + 1] - toff[h];
+        if (nt == 0) continue;
+        const int own = ct.owner_of_new(u);
+        for (int i = 0; i < nt; i++) {
+            const int pb = b + i * task_pairs;
+            const int pe = pb + task_pairs < e ? pb + task_pairs : e;
+            tasks[toff[h] + i] = make_int4(u, pb, pe, (nt << 1) | own);
+        }
+    }
+}
+
+template <class T>
+__global__ void k_task_reset(int heavy_begin, int n_pad, const int *toff, ClassTable ct, T *hacc, int *hrem)
+{
+    const int nh = n_pad - heavy_begin;
+    for (long long h = (long long)blockIdx.x * blockDim.x + threadIdx.x; h < nh; h += (long long)gridDim.x * blockDim.x) {
+        const int u = heavy_begin + (int)h;
+        hrem[h] = toff[h + 1] - toff[h];
+        hacc[h] = ct.owner_of_new(u) ? (T)0 : credit_traits<T>::top;
+    }
+}
+
+void launch_task_reset(int bits, int heavy_begin, int n_pad, const int *toff, ClassTable ct, void *hacc, int *hrem,
+                       cudaStream_t st)
+{
+    const long long nh = n_pad - heavy_begin;
+    long long g = (nh + 255) / 256;
+    g = g < 1 ? 1 : (g > 148 * 32 ? 148 * 32 : g);
+    if (bits == 32) k_task_reset<int32_t><<<(unsigned)g, 256, 0, st>>>(heavy_begin, n_pad, toff, ct, (int32_t *)hacc, hrem);
+    else k_task_reset<int64_t><<<(unsigned)g, 256, 0, st>>>(heavy_begin, n_pad, toff, ct, (int64_t *)hacc, hrem);
+}
+
 /* Credits back in original vertex order (and width). */
 template <class T, class O>
 __global__ void k_gather_out(int n, const int *iperm, const T *F, O *out)

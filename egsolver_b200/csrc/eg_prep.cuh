@@ -48,6 +48,13 @@ __global__ void k_copy_edges(int n_pad, const int *perm, const int *iperm, const
                              const int *w, const int *P, int2 *E, int *csc_key, int *csc_val, int *indeg,
                              ClassTable ct, int topv, int zerov);
 __global__ void k_init_frontier(int n_pad, const int *perm, const unsigned char *active0, uint32_t *B);
+/* heavy tasks: per heavy vertex the number of 256-edge tasks, then the tasks */
+__global__ void k_task_count(int heavy_begin, int n_pad, const int *P, int task_pairs, int *count);
+__global__ void k_task_fill(int heavy_begin, int n_pad, const int *P, int task_pairs, const int *toff, ClassTable ct,
+                            int4 *tasks);
+/* per solve: tasks-to-report counters and identity partials */
+void launch_task_reset(int bits, int heavy_begin, int n_pad, const int *toff, ClassTable ct, void *hacc, int *hrem,
+                       cudaStream_t st);
 /* credits: 0 everywhere except TOP at the sentinel topv */
 void launch_init_credits(int bits, int n_alloc, void *F, int topv, cudaStream_t st);
 /* number of TOP credits among the first n_pad, added to *out */

@@ -42,3 +42,22 @@ def cfg4_thresholds(num_games: int = 4096, k: int = 8, seed: int = SEED + 4):
 
     rng = np.random.default_rng(seed + 1)
     return rng.integers(-800, 801, size=(num_games, k)).astype(np.int32), 8
+
+
+def cfg5_requests(num: int, n_max: int = 1 << 22, seed: int = SEED + 5):
+    """Served workload: request games with n log-uniform in [1000, n_max]
+    (4M in the configuration), out-degree 1 + geometric (mean 6), owners
+    50/50, weights uniform in [-W, W] with W log-uniform in [10, 10^4]; each
+    request carries K in {4..32} thresholds p uniform in [-8W, 8W] at d = 8."""
+    import numpy as np
+
+    rng = np.random.default_rng(seed)
+    out = []
+    for i in range(num):
+        n = int(round(float(np.exp(rng.uniform(np.log(1000), np.log(n_max))))))
+        W = int(round(float(np.exp(rng.uniform(np.log(10), np.log(10_000))))))
+        K = int(rng.integers(4, 33))
+        p = rng.integers(-8 * W, 8 * W + 1, size=K).astype(np.int32)
+        g = generate(5, n, min(256, n - 1), W, seed * 7_919 + i, param=6)
+        out.append((g, p, 8))
+    return out

@@ -99,7 +99,9 @@ typedef struct eg_opts {
                                     vertex (reference --shuffling K); 0 means 32       */
     int32_t keep_layout;         /* non-zero: reuse the transpose/renumbering of the
                                     previous solve of the same resident game           */
-    int32_t reserved[5];
+    int32_t grid_ctas;           /* cap on the lifting grid's CTAs (0: every SM, full
+                                    occupancy); a smaller grid leaves SMs to other work */
+    int32_t reserved[4];
 } eg_opts;
 
 typedef struct eg_stats {

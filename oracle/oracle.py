@@ -44,7 +44,8 @@ _ref = None
 def ensure_built() -> None:
     if not LIB.exists() or LIB.stat().st_mtime < (HERE / "eg_oracle.c").stat().st_mtime:
         subprocess.run(["make", "-C", str(HERE), "all"], check=True, capture_output=True)
-    if (REF_TREE / "src" / "cpu_solver.c").exists() and not REF_LIB.exists():
+    if (REF_TREE / "src" / "cpu_solver.c").exists():
+        # incremental: relinks the reference driver whenever the solver library changed
         subprocess.run(["make", "-C", str(HERE), "ref", f"REF={REF_TREE}"], check=True, capture_output=True)
 
 

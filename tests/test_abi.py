@@ -14,7 +14,7 @@ from egsolver_b200 import _ffi, workloads
 from oracle import oracle as O
 from tests.conftest import ROOT
 
-HEADER = ROOT / "include" / "egsolver_b200.h"
+HEADERS = [ROOT / "include" / "egsolver_b200.h", ROOT / "include" / "egsolver_b200_serve.h"]
 
 REFERENCE_ABI = ["alloca_memoria_host", "alloca_memoria_device", "copia_dati_su_device", "gpu_solver",
                  "dealloca_memoria_host", "dealloca_memoria_device", "checkDevice", "checkCUDAError"]
@@ -34,7 +34,7 @@ def exported(lib_path) -> set[str]:
 
 
 def test_every_declared_function_is_exported_and_bound():
-    decl = declared_functions(HEADER)
+    decl = set().union(*(declared_functions(h) for h in HEADERS))
     assert len(decl) >= 25, decl
     exp = exported(_ffi.LIB_PATH)
     missing = decl - exp

@@ -1,0 +1,111 @@
+"""GPU tests of the serving loop: results in the mix equal results alone,
+admission by free device memory, the large-game path, statistics."""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+import egsolver_b200 as eg
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+
+def mixed_games(num=16, seed=13):
+    rng = np.random.default_rng(seed)
+    out = []
+    for i in range(num):
+        n = int(np.exp(rng.uniform(np.log(60), np.log(3000))))
+        out.append(eg.generate(5, n, min(60, n - 1), int(rng.integers(5, 40)), 500 + i, param=6))
+    return out
+
+
+def alone(game, p, d):
+    """The same query solved alone, outside the server (batched kernel, one game)."""
+    with eg.Batch([game], thresholds=len(p), scale=d) as b:
+        b.set_thresholds(np.asarray(p, np.int32).reshape(1, -1))
+        b.solve()
+        return b.credits(0)
+
+
+def test_results_in_the_mix_equal_results_alone():
+    games = mixed_games()
+    rng = np.random.default_rng(1)
+    d = 8
+    with eg.Server(streams=3) as srv:
+        gids = [srv.add_game(g) for g in games]
+        queries = []
+        for rep in range(3):  # several queries per game: the game stays resident
+            for gi, gid in enumerate(gids):
+                K = int(rng.integers(1, 9))
+                W = int(np.abs(games[gi].weight).max())
+                p = rng.integers(-8 * W, 8 * W + 1, size=K).astype(np.int32)
+                queries.append((srv.submit(gid, p, d), gi, p))
+        for qid, gi, p in queries:
+            srv.wait(qid, 120_000)
+        for qid, gi, p in queries:
+            got, _ = srv.result(qid)
+            np.testing.assert_array_equal(got, alone(games[gi], p, d))
+        st = srv.stats()
+        assert st["completed"] == len(queries) and st["failed"] == 0
+        assert st["game_uploads"] == len(games)  # uploaded once, reused across queries
+        assert st["latency_p99_ms"] >= st["latency_p50_ms"] > 0
+        assert st["micro_batches"] >= 1
+
+
+def test_served_results_match_the_oracle():
+    games = mixed_games(4, seed=3)
+    with eg.Server() as srv:
+        for g in games:
+            gid = srv.add_game(g)
+            p = np.array([-40, 0, 25], dtype=np.int32)
+            qid = srv.submit(gid, p, 4)
+            srv.wait(qid, 60_000)
+            got, _ = srv.result(qid)
+            for k in range(3):
+                want, _ = O.eg_solve(eg.threshold_game(g, int(p[k]), 4), bits=64)
+                np.testing.assert_array_equal(got[k], want)
+
+
+def test_large_game_runs_on_the_grid_path():
+    n = (1 << 19) + 4096
+    g = eg.generate(1, n, 3, 4, 99)
+    p = np.array([-3, 1], dtype=np.int32)
+    with eg.Server(large_ctas=74) as srv:
+        gid = srv.add_game(g)
+        small = mixed_games(3, seed=8)
+        sids = [srv.add_game(x) for x in small]
+        qid = srv.submit(gid, p, 2)
+        others = [srv.submit(s, np.array([0, 3], np.int32), 2) for s in sids]
+        srv.wait(qid, 300_000)
+        got, _ = srv.result(qid)
+        for k in range(2):
+            want, _ = eg.solve(eg.threshold_game(g, int(p[k]), 2))
+            np.testing.assert_array_equal(got[k], want)
+        for s, q in zip(small, others):
+            srv.wait(q, 60_000)
+            r, _ = srv.result(q)
+            np.testing.assert_array_equal(r, alone(s, [0, 3], 2))
+
+
+def test_admission_refuses_what_can_never_fit():
+    g = mixed_games(1)[0]
+    with eg.Server(hbm_reserve_bytes=1 << 60) as srv:  # nothing may be used
+        gid = srv.add_game(g)
+        qid = srv.submit(gid, np.array([0], np.int32), 1)
+        srv.wait(qid, 30_000)
+        state, _ = srv.poll(qid)
+        assert state == 3  # EG_QUERY_FAILED
+        with pytest.raises(eg.EGError) as ei:
+            srv.result(qid)
+        assert ei.value.name == "EG_ERR_OOM"
+
+
+def test_unknown_game_and_bad_arguments():
+    with eg.Server() as srv:
+        with pytest.raises(eg.EGError) as ei:
+            srv.submit(12345, [0])
+        assert ei.value.name == "EG_ERR_NOT_FOUND"
+        gid = srv.add_game(mixed_games(1)[0])
+        with pytest.raises(eg.EGError):
+            srv.submit(gid, np.zeros(40, np.int32))  # K > 32
