@@ -200,6 +200,7 @@ SIGNATURES = {
     "eg_batch_tune": (_I32, [_P, C.POINTER(_I32)]),
     "eg_batch_device_bytes": (_I64, [_P]),
     "eg_batch_free": (None, [_P]),
+    "eg_csr2csc_device_noalloc": (_I32, [_I32, _I32, _I64, _P, _P, _P, _P, _P, _P, _P]),
     "eg_serve_create": (_I32, [C.POINTER(EgServeOpts), C.POINTER(_P)]),
     "eg_serve_add_game": (_I32, [_P, C.POINTER(EgGame), C.POINTER(_I64)]),
     "eg_serve_remove_game": (_I32, [_P, _I64]),

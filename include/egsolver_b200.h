@@ -259,6 +259,29 @@ int64_t eg_batch_device_bytes(const eg_batch *b);
 void eg_batch_free(eg_batch *b);
 
 /* ------------------------------------------------------------------ */
+/* Allocation-free transpose                                            */
+/* ------------------------------------------------------------------ */
+
+/* No counterpart in the reference.  The same transpose as eg_csr2csc_i32,
+ * for callers that cannot allocate device memory when they need it (code
+ * running during CUDA stream capture, runtimes that own all device memory
+ * in their own pool, hosts that forbid allocation after start-up).  All
+ * pointers are device pointers owned by the caller; stream is a
+ * cudaStream_t (NULL: the legacy default stream).  Temporaries live in one
+ * static device array sized for EG_NOALLOC_MAX_NNZ entries and
+ * EG_NOALLOC_MAX_COLS columns (about 25 MB, held by every GPU that loads the
+ * library until exit); larger inputs are rejected with EG_ERR_INVALID.  The
+ * call never allocates, and returns after the transpose has finished on the
+ * stream.  The first call on each device looks the static array up
+ * (cudaGetSymbolAddress), so make it before any stream capture.  Calls that
+ * overlap on the GPU share the array and race; serialise them. */
+#define EG_NOALLOC_MAX_NNZ (1LL << 20)
+#define EG_NOALLOC_MAX_COLS (1LL << 20)
+eg_status eg_csr2csc_device_noalloc(int32_t num_rows, int32_t num_cols, int64_t nnz,
+                                    const int64_t *row_ptr, const int32_t *col_idx, const int32_t *val,
+                                    int64_t *csc_ptr, int32_t *csc_row, int32_t *csc_val, void *stream);
+
+/* ------------------------------------------------------------------ */
 /* Cancellation                                                         */
 /* ------------------------------------------------------------------ */
 
