@@ -122,6 +122,9 @@ class Stats:
     pushes: int
     grid: int
     block: int
+    phase_heavy_ns: float
+    phase_light_ns: float
+    phase_wait_ns: float
 
     @classmethod
     def from_c(cls, s: _ffi.EgStats) -> "Stats":
@@ -134,7 +137,8 @@ class Stats:
 
 def make_opts(credit_bits: int = 64, variant: int = VARIANT_AUTO, max_rounds: int = -1, timeout_ms: float = 0.0,
               device: int = 0, lanes_per_vertex: int = 0, small_max_deg: int = 0, large_min_deg: int = 0,
-              keep_layout: bool = False, cancel: Optional["CancelFlag"] = None, grid_ctas: int = 0) -> _ffi.EgOpts:
+              keep_layout: bool = False, cancel: Optional["CancelFlag"] = None, grid_ctas: int = 0,
+              task_edges: int = 0, schedule: int = 0, profile: bool = False, ctas_per_sm: int = 0) -> _ffi.EgOpts:
     o = _ffi.EgOpts()
     lib().eg_opts_default(C.byref(o))
     o.credit_bits = credit_bits
@@ -147,6 +151,10 @@ def make_opts(credit_bits: int = 64, variant: int = VARIANT_AUTO, max_rounds: in
     o.large_min_deg = large_min_deg
     o.keep_layout = 1 if keep_layout else 0
     o.grid_ctas = grid_ctas
+    o.task_edges = task_edges
+    o.schedule = schedule
+    o.profile = 1 if profile else 0
+    o.ctas_per_sm = ctas_per_sm
     o.cancel = cancel.ptr if cancel is not None else None
     return o
 

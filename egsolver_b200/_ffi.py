@@ -48,7 +48,10 @@ class EgOpts(C.Structure):
         ("lanes_per_vertex", C.c_int32),
         ("keep_layout", C.c_int32),
         ("grid_ctas", C.c_int32),
-        ("reserved", C.c_int32 * 4),
+        ("task_edges", C.c_int32),
+        ("schedule", C.c_int32),
+        ("profile", C.c_int32),
+        ("ctas_per_sm", C.c_int32),
     ]
 
 
@@ -73,6 +76,9 @@ class EgStats(C.Structure):
         ("grid", C.c_int32),
         ("block", C.c_int32),
         ("reserved", C.c_int32 * 2),
+        ("phase_heavy_ns", C.c_double),
+        ("phase_light_ns", C.c_double),
+        ("phase_wait_ns", C.c_double),
     ]
 
     def as_dict(self) -> dict:

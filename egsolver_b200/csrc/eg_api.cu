@@ -90,7 +90,7 @@ struct eg_dgame {
     void *d_hacc;
     int *d_hrem, *d_toff;
     long long task_cap;
-    int num_tasks, heavy_begin, heavy_bucket;
+    int num_tasks, heavy_begin, heavy_bucket, task_pairs;
     size_t bytes;
     long long mg;
     int solved_bits;
@@ -121,13 +121,33 @@ extern "C" eg_status eg_device_count(int32_t *count)
     return EG_OK;
 }
 
-/* Degree buckets and the lane-group size of each bucket.  AUTO: deg <= 8
- * thread-per-vertex, 9..64 eight lanes, 65..1023 a warp, >= 1024 a CTA. */
+/* Degree buckets and the lane-group size of each bucket.
+ * AUTO / SMEM: deg <= small_max_deg (8) thread-per-vertex, up to
+ * large_min_deg - 1 (64) eight lanes, from large_min_deg (65) on "heavy":
+ * cut into edge tasks on the grid, a warp per vertex in the one-CTA kernel.
+ * Forced variants keep the reference-style buckets below. */
 static void choose_layout(const eg_opts *o, BucketBounds *bb, int *groups)
 {
+    const int v = o ? o->variant : EG_VARIANT_AUTO;
+    if (v == EG_VARIANT_AUTO || v == EG_VARIANT_SMEM) {
+        /* light vertices (deg < large_min_deg, default 17) in warp-cooperative
+         * words; heavy ones as edge tasks (a warp each in the one-CTA kernel).
+         * small_max_deg > 0 splits off a thread-per-vertex bucket. */
+        const int heavy = o && o->large_min_deg > 1 ? o->large_min_deg : 17;
+        const int small = o && o->small_max_deg > 0 ? o->small_max_deg : 0;
+        int nb = 0;
+        if (small > 0 && small < heavy - 1) {
+            bb->upper[nb] = small;
+            groups[nb++] = 1;
+        }
+        bb->upper[nb] = heavy - 1;
+        groups[nb++] = EG_GROUP_LIGHT;
+        groups[nb++] = 32;
+        bb->nb = nb;
+        return;
+    }
     const int small = o && o->small_max_deg > 0 ? o->small_max_deg : 8;
     const int large = o && o->large_min_deg > 0 ? o->large_min_deg : 1024;
-    const int v = o ? o->variant : EG_VARIANT_AUTO;
     if (v == EG_VARIANT_THREAD || v == EG_VARIANT_WARP || v == EG_VARIANT_CTA) {
         bb->nb = 1;
         int g = 1;
@@ -243,7 +263,7 @@ static eg_status dgame_alloc(const eg_game *game, const eg_opts *opts, eg_dgame 
     if (s == EG_OK) s = dalloc(g, &g->d_iperm, (size_t)g->n);
     if (s == EG_OK) s = dalloc(g, &g->d_P, (size_t)g->n_pad_cap + 1);
     if (s == EG_OK) s = dalloc(g, &g->d_CP, (size_t)g->n_pad_cap + 1);
-    if (s == EG_OK) s = dalloc(g, &g->d_CS, (size_t)g->m);
+    if (s == EG_OK) s = dalloc(g, &g->d_CS, (size_t)g->m + 3 * (size_t)g->n_pad_cap + 8);
     if (s == EG_OK) s = dalloc(g, &g->d_E, (size_t)g->m_pad_cap);
     if (s == EG_OK) s = dalloc(g, &g->d_active0, (size_t)g->n);
     if (s == EG_OK) s = dalloc(g, &g->d_k0, (size_t)g->tmp_cap);
@@ -257,7 +277,7 @@ static eg_status dgame_alloc(const eg_game *game, const eg_opts *opts, eg_dgame 
     if (s == EG_OK) s = dalloc(g, (int64_t **)&g->d_out, (size_t)g->n);
     if (s == EG_OK) s = dalloc(g, &g->d_B, (size_t)(2 * words));
     if (s == EG_OK) s = dalloc(g, &g->d_ctrl, 1);
-    g->task_cap = g->m_pad_cap / (2 * kTaskPairs) + g->n_pad_cap + 2;
+    g->task_cap = g->m_pad_cap / 32 + g->n_pad_cap + 2; /* tasks of >= 16 pairs */
     if (s == EG_OK) s = dalloc(g, &g->d_tasks, (size_t)g->task_cap);
     if (s == EG_OK) s = dalloc(g, (int64_t **)&g->d_hacc, (size_t)g->n_pad_cap);
     if (s == EG_OK) s = dalloc(g, &g->d_hrem, (size_t)g->n_pad_cap);
@@ -375,9 +395,13 @@ static eg_status dgame_prepare(eg_dgame *g, const eg_opts *opts)
     k_copy_edges<<<grid_for((long long)n_pad * 32, kPrepBlock), kPrepBlock, 0, st>>>(
         n_pad, g->d_perm, g->d_iperm, g->d_rowptr, g->d_succ, g->d_w, g->d_P, g->d_E, g->d_k0, g->d_v0, g->d_CP, ct,
         n_pad, n_pad + 1);
+    /* padded predecessor offsets (d_hrem serves as temporary: n_pad + 1 ints) */
+    k_round4<<<grid_for(n_pad + 1, kPrepBlock), kPrepBlock, 0, st>>>(n_pad + 1, g->d_CP, g->d_hrem);
     excl_scan(g->d_CP, (long long)n_pad + 1, g->d_scratch, st);
+    excl_scan(g->d_hrem, (long long)n_pad + 1, g->d_scratch, st);
     radix_sort_pairs(g->d_k0, g->d_v0, g->d_k1, g->d_v1, g->m, bits_for(n_pad + 1), g->d_scratch, st, &sk, &sv);
-    EG_CUDA(cudaMemcpyAsync(g->d_CS, sv, sizeof(int) * (size_t)g->m, cudaMemcpyDeviceToDevice, st));
+    k_csc_pad<<<grid_for((long long)n_pad * 32, kPrepBlock), kPrepBlock, 0, st>>>(n_pad, g->d_CP, g->d_hrem, sv, g->d_CS);
+    EG_CUDA(cudaMemcpyAsync(g->d_CP, g->d_hrem, sizeof(int) * ((size_t)n_pad + 1), cudaMemcpyDeviceToDevice, st));
     g->launches += 8 + 3 * ((bits_for(n_pad + 1) + 7) / 8) * 2;
     /* AUTO layout: vertices of the warp / CTA buckets become 256-edge tasks */
     g->num_tasks = 0;
@@ -393,14 +417,16 @@ static eg_status dgame_prepare(eg_dgame *g, const eg_opts *opts)
             g->heavy_begin = ct.start[2 * g->heavy_bucket];
             const int nh = n_pad - g->heavy_begin;
             if (nh > 0) {
-                k_task_count<<<grid_for(nh + 1, kPrepBlock), kPrepBlock, 0, st>>>(g->heavy_begin, n_pad, g->d_P, kTaskPairs,
+                const int tp = opts && opts->task_edges > 0 ? std::min(kTaskPairs, std::max(16, opts->task_edges / 2)) : kTaskPairs;
+                g->task_pairs = tp;
+                k_task_count<<<grid_for(nh + 1, kPrepBlock), kPrepBlock, 0, st>>>(g->heavy_begin, n_pad, g->d_P, tp,
                                                                                    g->d_toff);
                 excl_scan(g->d_toff, (long long)nh + 1, g->d_scratch, st);
                 int total = 0;
                 EG_CUDA(cudaMemcpyAsync(&total, g->d_toff + nh, sizeof total, cudaMemcpyDeviceToHost, st));
                 EG_CUDA(cudaStreamSynchronize(st));
                 if (total > g->task_cap) return eg_set_error(EG_ERR_INVALID, "task list overflow (%d tasks)", total);
-                k_task_fill<<<grid_for(nh, kPrepBlock), kPrepBlock, 0, st>>>(g->heavy_begin, n_pad, g->d_P, kTaskPairs,
+                k_task_fill<<<grid_for(nh, kPrepBlock), kPrepBlock, 0, st>>>(g->heavy_begin, n_pad, g->d_P, tp,
                                                                                g->d_toff, ct, g->d_tasks);
                 g->num_tasks = total;
                 g->launches += 5;
@@ -458,6 +484,7 @@ extern "C" eg_status eg_dgame_solve(eg_dgame *g, const eg_opts *opts_in, eg_stat
         p.cancel = (const int *)dp;
     }
     p.n_pad = n_pad;
+    p.profile = opts->profile != 0;
     const bool small = n_pad <= kSmallGameMaxPad &&
                        (opts->variant == EG_VARIANT_SMEM || (opts->variant == EG_VARIANT_AUTO && g->m <= kSmallGameEdges));
     /* the grid kernel lifts heavy buckets as tasks; the one-CTA kernel
@@ -474,10 +501,12 @@ extern "C" eg_status eg_dgame_solve(eg_dgame *g, const eg_opts *opts_in, eg_stat
             lc.word_end = (g->ct.start[c] + g->ct.count[c] + 31) / 32;
             lc.owner = own;
             lc.group = g->groups[b];
-            lc.grab = g->groups[b] == 1 ? 2 : 1;
+            lc.grab = g->groups[b] == 1 ? (opts->schedule == 1 ? -4 : 2) : 1;
         }
     }
     p.nclasses = nc;
+    p.lean = tasks && (opts->variant == EG_VARIANT_AUTO || opts->variant == EG_VARIANT_SMEM) && opts->ctas_per_sm != 2 &&
+             opts->small_max_deg <= 0; /* the lean kernel knows only light words and tasks */
     if (tasks) {
         launch_task_reset(bits, g->heavy_begin, n_pad, g->d_toff, g->ct, g->d_hacc, g->d_hrem, st);
         g->launches++;
@@ -529,6 +558,13 @@ extern "C" eg_status eg_dgame_solve(eg_dgame *g, const eg_opts *opts_in, eg_stat
         stats->pushes = (int64_t)ctrl.pushes;
         stats->grid = grid;
         stats->block = block;
+        if (p.profile) {
+            /* average per warp and round, in nanoseconds */
+            const double wr = (double)grid * (block / 32) * (double)(ctrl.rounds ? ctrl.rounds : 1);
+            stats->phase_heavy_ns = ctrl.t_heavy / wr;
+            stats->phase_light_ns = ctrl.t_light / wr;
+            stats->phase_wait_ns = ctrl.t_wait / wr;
+        }
     }
     if (ctrl.stop == EG_ERR_LOOPCAP)
         return eg_set_error(EG_ERR_LOOPCAP, "round cap %lld reached with work left", (long long)opts->max_rounds);

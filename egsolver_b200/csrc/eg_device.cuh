@@ -66,14 +66,28 @@ __device__ __forceinline__ bool bitmap_push(uint32_t *bm, int32_t p)
     return !(atomicOr(w, mask) & mask);
 }
 
-/* Sets bit p of a frontier bitmap without waiting for the old word (a
- * reduction, not a fetch): the caller decides "the next round has work"
- * from the raise itself, so the atomic's latency is off the critical path. */
+/* Sets bit p of a frontier bitmap.  Most pushes in a dense round find the
+ * bit already set, so an L2 read filters them before the atomic: frontier
+ * words are hot and atomics on one word serialise.  The atomic's result is
+ * not needed (the caller decides "the next round has work" from the raise
+ * itself), so it is issued as a reduction. */
 __device__ __forceinline__ void bitmap_mark(uint32_t *bm, int32_t p)
 {
     const uint32_t mask = 1u << (p & 31);
     uint32_t *w = bm + (p >> 5);
     if (!(__ldcg(w) & mask)) atomicOr(w, mask);
+}
+
+/* Pushes the four predecessors of one 128-bit load of a padded list;
+ * returns how many were real (not padding). */
+template <class Pol>
+__device__ __forceinline__ unsigned push4(const Pol &pol, const int4 c)
+{
+    if (c.x >= 0) pol.push(c.x);
+    if (c.y >= 0) pol.push(c.y);
+    if (c.z >= 0) pol.push(c.z);
+    if (c.w >= 0) pol.push(c.w);
+    return (unsigned)(c.x >= 0) + (c.y >= 0) + (c.z >= 0) + (c.w >= 0);
 }
 
 /* Control block of a persistent solve.  Counters that a round uses are
@@ -94,6 +108,14 @@ struct Ctrl {
     unsigned long long num_top;        /* vertices at TOP after the solve            */
     unsigned long long changes;        /* lifts that raised a credit                 */
     unsigned long long pushes;         /* predecessor entries scanned                */
+    /* phase timers (diagnostic mode): warp-nanoseconds summed over warps and
+     * rounds in heavy tasks, in word classes, and waiting at the barrier */
+    unsigned long long t_heavy, t_light, t_wait;
+    /* direction switching */
+    unsigned long long round_changes[2]; /* raises of round r, by parity         */
+    int next_mode;                       /* 0 sparse, 1 dense, 2 seed then sparse */
+    int pad2;
+    long long dense_rounds;
 };
 
 /* Grid barrier for a cooperative launch.  Every wait is bounded by

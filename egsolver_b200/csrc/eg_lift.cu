@@ -140,11 +140,9 @@ __device__ __forceinline__ void lift_group(const LiftParams &p, T *F, const Pol 
             pol.store(F + u, acc);
             cnt.changes++;
         }
-        const int cb = __ldg(p.CP + u), ce = __ldg(p.CP + u + 1);
-        if (gl == 0) cnt.pushes += (unsigned)(ce - cb);
+        const int cb = __ldg(p.CP + u) >> 2, ce = __ldg(p.CP + u + 1) >> 2;
         cnt.any_new |= ce > cb;
-#pragma unroll 4
-        for (int k = cb + gl; k < ce; k += G) pol.push(__ldg(p.CS + k));
+        for (int k = cb + gl; k < ce; k += G) cnt.pushes += push4(pol, __ldg((const int4 *)p.CS + k));
     }
     if (gl == 0) cnt.lifts++;
 }
@@ -200,16 +198,26 @@ __device__ __noinline__ void warp_class(const LiftParams &p, const LiftClass &lc
  * those words through each load phase together. */
 template <class T, int OWNER>
 __device__ __noinline__ void thread_class(const LiftParams &p, const LiftClass &lc, T *F, uint32_t *cur, uint32_t *nxt,
-                                          LiftCounters &cnt)
+                                          int *ctr, LiftCounters &cnt)
 {
     constexpr int U = 4;
     const int lane = threadIdx.x & 31;
     const int gwarp = (int)((blockIdx.x * (unsigned)blockDim.x + threadIdx.x) >> 5);
     const int nwarp = (int)((gridDim.x * (unsigned)blockDim.x) >> 5);
     const int nwords = lc.word_end - lc.word_begin;
-    /* every warp gets the same number of words (+-1) of this class */
-    const int lo = (int)((long long)gwarp * nwords / nwarp), hi = (int)((long long)(gwarp + 1) * nwords / nwarp);
-    for (int w0 = lo; w0 < hi; w0 += U) {
+    /* static: every warp gets the same number of words (+-1) of the class;
+     * dynamic (grab < 0): warps take U words at a time in increasing order,
+     * so later words see credits raised earlier in the same round */
+    const bool dyn = lc.grab < 0;
+    const int lo = dyn ? 0 : (int)((long long)gwarp * nwords / nwarp);
+    const int hi = dyn ? nwords : (int)((long long)(gwarp + 1) * nwords / nwarp);
+    for (int w0 = lo;; w0 += U) {
+        if (dyn) {
+            int t = 0;
+            if (lane == 0) t = atomicAdd(ctr, U);
+            w0 = __shfl_sync(0xffffffffu, t, 0);
+        }
+        if (w0 >= hi) break;
         uint32_t mine = 0;
         if (lane < U && w0 + lane < hi) {
             uint32_t *wp = cur + lc.word_begin + w0 + lane;
@@ -255,11 +263,10 @@ __device__ __noinline__ void thread_class(const LiftParams &p, const LiftClass &
                 if (old[j] < acc[j]) {
                     st_credit(F + u[j], acc[j]);
                     cnt.changes++;
-                    const int cb = __ldg(p.CP + u[j]), ce = __ldg(p.CP + u[j] + 1);
-                    cnt.pushes += (unsigned)(ce - cb);
+                    const int cb = __ldg(p.CP + u[j]) >> 2, ce = __ldg(p.CP + u[j] + 1) >> 2;
                     cnt.any_new |= ce > cb;
-#pragma unroll 4
-                    for (int k = cb; k < ce; k++) bitmap_mark(nxt, __ldg(p.CS + k));
+                    const GridPolicy pol{nxt};
+                    for (int k = cb; k < ce; k++) cnt.pushes += push4(pol, __ldg((const int4 *)p.CS + k));
                 }
             }
         }
@@ -303,10 +310,10 @@ __device__ __forceinline__ void heavy_finalize(const LiftParams &p, T *F, uint32
     }
     raise = __shfl_sync(0xffffffffu, raise, 0);
     if (raise) {
-        const int cb = __ldg(p.CP + u), ce = __ldg(p.CP + u + 1);
-        if (lane == 0) cnt.pushes += (unsigned)(ce - cb);
+        const int cb = __ldg(p.CP + u) >> 2, ce = __ldg(p.CP + u + 1) >> 2;
         cnt.any_new |= ce > cb;
-        for (int k = cb + lane; k < ce; k += 32) bitmap_mark(nxt, __ldg(p.CS + k));
+        const GridPolicy pol{nxt};
+        for (int k = cb + lane; k < ce; k += 32) cnt.pushes += push4(pol, __ldg((const int4 *)p.CS + k));
     }
 }
 
@@ -373,6 +380,246 @@ __device__ __noinline__ void heavy_tasks(const LiftParams &p, T *F, uint32_t *cu
     }
 }
 
+/* Lane index of the last entry of a warp-wide exclusive scan `excl` whose
+ * value is <= t (the owner of item t): binary search by shuffles.  Every
+ * lane of the warp must call it. */
+__device__ __forceinline__ int owner_of(int excl, int t)
+{
+    int lo = 0;
+#pragma unroll
+    for (int step = 16; step > 0; step >>= 1) {
+        const int mid = lo + step;
+        const int e = __shfl_sync(0xffffffffu, excl, mid & 31);
+        if (mid < 32 && e <= t) lo = mid;
+    }
+    return lo;
+}
+
+__device__ __forceinline__ int warp_excl_scan(int v, int lane, int *total)
+{
+    int incl = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int t = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += t;
+    }
+    *total = __shfl_sync(0xffffffffu, incl, 31);
+    return incl - v;
+}
+
+/* One frontier word of light vertices, warp-cooperative and edge-parallel:
+ * lane j owns vertex j of the word; the word's edge pairs are dealt to the
+ * 32 lanes, combined per vertex by a segmented shuffle reduction, and the
+ * predecessor lists of the raised vertices are pushed the same way, four
+ * per 128-bit load.  The dependent memory steps per word do not depend on
+ * the vertices' degrees. */
+template <class T, int OWNER, class Pol>
+__device__ __forceinline__ void light_word(const LiftParams &p, T *F, const Pol &pol, int gw, uint32_t word, int lane,
+                                           LiftCounters &cnt)
+{
+    const int u = (gw << 5) + lane;
+    const bool act = (word >> lane) & 1u;
+    int b = 0, np = 0;
+    T old = (T)0;
+    if (act) {
+        b = __ldg(p.P + u) >> 1;
+        np = (__ldg(p.P + u + 1) >> 1) - b;
+        old = pol.load(F + u);
+    }
+    int total;
+    const int excl = warp_excl_scan(np, lane, &total);
+    T acc = identity<OWNER, T>();
+    int real = 0;
+    for (int base = 0; base < total; base += 32) {
+        const int t = base + lane;
+        const int own = owner_of(excl, t);
+        const int ob = __shfl_sync(0xffffffffu, b, own);
+        const int oe = __shfl_sync(0xffffffffu, excl, own);
+        T val = identity<OWNER, T>();
+        if (t < total) {
+            const int4 q = __ldg(p.E4 + ob + (t - oe));
+            const T v0 = ominus<T>(pol.load(F + q.x), q.y, p.mg);
+            const T v1 = ominus<T>(pol.load(F + q.z), q.w, p.mg);
+            val = combine<OWNER>(v0, v1);
+            real += 1 + (q.z < p.n_pad);
+        }
+        /* segmented inclusive min / max over runs of equal owner */
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const T other = shfl_idx<T>(0xffffffffu, val, (lane - o) & 31, 32);
+            const int oo = __shfl_sync(0xffffffffu, own, (lane - o) & 31);
+            if (lane >= o && oo == own) val = combine<OWNER>(val, other);
+        }
+        /* vertex j takes the value of the last lane of its run in this chunk */
+        const int s0 = excl > base ? excl : base;
+        const int s1 = (excl + np < base + 32 ? excl + np : base + 32) - 1;
+        const T mine = shfl_idx<T>(0xffffffffu, val, (s1 - base) & 31, 32);
+        if (np > 0 && s0 <= s1) acc = combine<OWNER>(acc, mine);
+    }
+    cnt.edges += (unsigned long long)real;
+    const bool raise = act && old < acc;
+    int cb = 0, nc = 0;
+    if (act) {
+        cnt.lifts++;
+        if (raise) {
+            pol.store(F + u, acc);
+            cnt.changes++;
+            cb = __ldg(p.CP + u) >> 2;
+            nc = (__ldg(p.CP + u + 1) >> 2) - cb;
+        }
+    }
+    int ptotal;
+    const int pexcl = warp_excl_scan(nc, lane, &ptotal);
+    cnt.any_new |= ptotal > 0;
+    for (int base = 0; base < ptotal; base += 32) {
+        const int t = base + lane;
+        const int own = owner_of(pexcl, t);
+        const int ocb = __shfl_sync(0xffffffffu, cb, own);
+        const int oex = __shfl_sync(0xffffffffu, pexcl, own);
+        if (t < ptotal) cnt.pushes += push4(pol, __ldg((const int4 *)p.CS + ocb + (t - oex)));
+    }
+}
+
+/* Two light words at once: the same steps as light_word, with the loads of
+ * both words issued together so that twice as many are in flight. */
+template <class T, int OWNER, class Pol>
+__device__ __forceinline__ void light_word2(const LiftParams &p, T *F, const Pol &pol, const int gw[2],
+                                            const uint32_t word[2], int lane, LiftCounters &cnt)
+{
+    int u[2], b[2], np[2], excl[2], total[2];
+    bool act[2];
+    T old[2], acc[2];
+#pragma unroll
+    for (int w = 0; w < 2; w++) {
+        u[w] = (gw[w] << 5) + lane;
+        act[w] = (word[w] >> lane) & 1u;
+        b[w] = 0;
+        np[w] = 0;
+        old[w] = (T)0;
+        acc[w] = identity<OWNER, T>();
+        if (act[w]) {
+            b[w] = __ldg(p.P + u[w]) >> 1;
+            np[w] = (__ldg(p.P + u[w] + 1) >> 1) - b[w];
+            old[w] = pol.load(F + u[w]);
+        }
+    }
+#pragma unroll
+    for (int w = 0; w < 2; w++) excl[w] = warp_excl_scan(np[w], lane, &total[w]);
+    const int tmax = total[0] > total[1] ? total[0] : total[1];
+    int real = 0;
+    for (int base = 0; base < tmax; base += 32) {
+        T val[2], f0[2], f1[2];
+        int own[2];
+        int4 q[2];
+        bool has[2];
+        /* phase 1: owners and edge pairs of both words */
+#pragma unroll
+        for (int w = 0; w < 2; w++) {
+            const int t = base + lane;
+            own[w] = owner_of(excl[w], t);
+            const int ob = __shfl_sync(0xffffffffu, b[w], own[w]);
+            const int oe = __shfl_sync(0xffffffffu, excl[w], own[w]);
+            has[w] = t < total[w];
+            q[w] = has[w] ? __ldg(p.E4 + ob + (t - oe)) : make_int4(0, 0, 0, 0);
+        }
+        /* phase 2: the successors' credits of both words */
+#pragma unroll
+        for (int w = 0; w < 2; w++) {
+            f0[w] = has[w] ? pol.load(F + q[w].x) : (T)0;
+            f1[w] = has[w] ? pol.load(F + q[w].z) : (T)0;
+        }
+#pragma unroll
+        for (int w = 0; w < 2; w++) {
+            val[w] = identity<OWNER, T>();
+            if (has[w]) {
+                val[w] = combine<OWNER>(ominus<T>(f0[w], q[w].y, p.mg), ominus<T>(f1[w], q[w].w, p.mg));
+                real += 1 + (q[w].z < p.n_pad);
+            }
+        }
+#pragma unroll
+        for (int w = 0; w < 2; w++) {
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const T other = shfl_idx<T>(0xffffffffu, val[w], (lane - o) & 31, 32);
+                const int oo = __shfl_sync(0xffffffffu, own[w], (lane - o) & 31);
+                if (lane >= o && oo == own[w]) val[w] = combine<OWNER>(val[w], other);
+            }
+            const int s0 = excl[w] > base ? excl[w] : base;
+            const int s1 = (excl[w] + np[w] < base + 32 ? excl[w] + np[w] : base + 32) - 1;
+            const T mine = shfl_idx<T>(0xffffffffu, val[w], (s1 - base) & 31, 32);
+            if (np[w] > 0 && s0 <= s1) acc[w] = combine<OWNER>(acc[w], mine);
+        }
+    }
+    cnt.edges += (unsigned long long)real;
+    int cb[2], nc[2], pexcl[2], ptotal[2];
+#pragma unroll
+    for (int w = 0; w < 2; w++) {
+        cb[w] = 0;
+        nc[w] = 0;
+        if (act[w]) {
+            cnt.lifts++;
+            if (old[w] < acc[w]) {
+                pol.store(F + u[w], acc[w]);
+                cnt.changes++;
+                cb[w] = __ldg(p.CP + u[w]) >> 2;
+                nc[w] = (__ldg(p.CP + u[w] + 1) >> 2) - cb[w];
+            }
+        }
+    }
+#pragma unroll
+    for (int w = 0; w < 2; w++) pexcl[w] = warp_excl_scan(nc[w], lane, &ptotal[w]);
+    cnt.any_new |= (ptotal[0] + ptotal[1]) > 0;
+    const int pmax = ptotal[0] > ptotal[1] ? ptotal[0] : ptotal[1];
+    for (int base = 0; base < pmax; base += 32) {
+#pragma unroll
+        for (int w = 0; w < 2; w++) {
+            const int t = base + lane;
+            const int own = owner_of(pexcl[w], t);
+            const int ocb = __shfl_sync(0xffffffffu, cb[w], own);
+            const int oex = __shfl_sync(0xffffffffu, pexcl[w], own);
+            if (t < ptotal[w]) cnt.pushes += push4(pol, __ldg((const int4 *)p.CS + ocb + (t - oex)));
+        }
+    }
+}
+
+/* Light words on the grid: dealt evenly to warps (static) or taken in
+ * order (schedule 1), two at a time. */
+template <class T, int OWNER>
+__device__ __noinline__ void light_class(const LiftParams &p, const LiftClass &lc, T *F, uint32_t *cur, uint32_t *nxt,
+                                         int *ctr, LiftCounters &cnt)
+{
+    const int lane = threadIdx.x & 31;
+    const int gwarp = (int)((blockIdx.x * (unsigned)blockDim.x + threadIdx.x) >> 5);
+    const int nwarp = (int)((gridDim.x * (unsigned)blockDim.x) >> 5);
+    const int nwords = lc.word_end - lc.word_begin;
+    const bool dyn = lc.grab < 0;
+    const int lo = dyn ? 0 : (int)((long long)gwarp * nwords / nwarp);
+    const int hi = dyn ? nwords : (int)((long long)(gwarp + 1) * nwords / nwarp);
+    const GridPolicy pol{nxt};
+    for (int w = lo;; w += 2) {
+        if (dyn) {
+            int t = 0;
+            if (lane == 0) t = atomicAdd(ctr, 2);
+            w = __shfl_sync(0xffffffffu, t, 0);
+        }
+        if (w >= hi) break;
+        int gw[2];
+        uint32_t word[2];
+        uint32_t mine = 0;
+        if (lane < 2 && w + lane < hi) {
+            uint32_t *wp = cur + lc.word_begin + w + lane;
+            mine = __ldcg(wp);
+            if (mine) __stcg(wp, 0u);
+        }
+#pragma unroll
+        for (int k = 0; k < 2; k++) {
+            gw[k] = lc.word_begin + w + k;
+            word[k] = __shfl_sync(0xffffffffu, mine, k);
+        }
+        if (word[0] | word[1]) light_word2<T, OWNER>(p, F, pol, gw, word, lane, cnt);
+    }
+}
+
 /* CTA-level processing: the whole CTA lifts one vertex at a time. */
 template <class T, int OWNER>
 __device__ __noinline__ void cta_class(const LiftParams &p, const LiftClass &lc, T *F, uint32_t *cur, uint32_t *nxt,
@@ -434,13 +681,11 @@ __device__ __noinline__ void cta_class(const LiftParams &p, const LiftClass &lc,
             }
             __syncthreads();
             if (s_raise) {
-                const int cb = __ldg(p.CP + u), ce = __ldg(p.CP + u + 1);
-                if (threadIdx.x == 0) {
-                    cnt.changes++;
-                    cnt.pushes += (unsigned)(ce - cb);
-                }
+                const int cb = __ldg(p.CP + u) >> 2, ce = __ldg(p.CP + u + 1) >> 2;
+                if (threadIdx.x == 0) cnt.changes++;
                 cnt.any_new |= ce > cb;
-                for (int k = cb + threadIdx.x; k < ce; k += LIFT_BLOCK) bitmap_mark(nxt, __ldg(p.CS + k));
+                const GridPolicy pol{nxt};
+                for (int k = cb + threadIdx.x; k < ce; k += LIFT_BLOCK) cnt.pushes += push4(pol, __ldg((const int4 *)p.CS + k));
             }
             if (threadIdx.x == 0) cnt.lifts++;
             __syncthreads();
@@ -448,13 +693,18 @@ __device__ __noinline__ void cta_class(const LiftParams &p, const LiftClass &lc,
     }
 }
 
-template <class T, int OWNER>
+template <class T, int OWNER, bool LEAN>
 __device__ __forceinline__ void run_class(const LiftParams &p, const LiftClass &lc, T *F, uint32_t *cur, uint32_t *nxt,
                                           int *ctr, LiftCounters &cnt)
 {
+    if (LEAN) { /* AUTO layout with heavy tasks: light classes only */
+        light_class<T, OWNER>(p, lc, F, cur, nxt, ctr, cnt);
+        return;
+    }
     switch (lc.group) {
+    case EG_GROUP_LIGHT: light_class<T, OWNER>(p, lc, F, cur, nxt, ctr, cnt); break;
     case EG_GROUP_CTA: cta_class<T, OWNER>(p, lc, F, cur, nxt, ctr, cnt); break;
-    case 1: thread_class<T, OWNER>(p, lc, F, cur, nxt, cnt); break;
+    case 1: thread_class<T, OWNER>(p, lc, F, cur, nxt, ctr, cnt); break;
     case 2: warp_class<T, 2, OWNER>(p, lc, F, cur, nxt, ctr, cnt); break;
     case 4: warp_class<T, 4, OWNER>(p, lc, F, cur, nxt, ctr, cnt); break;
     case 8: warp_class<T, 8, OWNER>(p, lc, F, cur, nxt, ctr, cnt); break;
@@ -463,8 +713,10 @@ __device__ __forceinline__ void run_class(const LiftParams &p, const LiftClass &
     }
 }
 
-template <class T>
-__global__ void __launch_bounds__(LIFT_BLOCK, 2) k_lift(const __grid_constant__ LiftParams p)
+/* LEAN: the AUTO layout only (heavy tasks, thread and 8-lane classes),
+ * compiled for three CTAs per SM; otherwise every variant, two CTAs per SM. */
+template <class T, bool LEAN>
+__global__ void __launch_bounds__(LIFT_BLOCK, LEAN ? 3 : 2) k_lift(const __grid_constant__ LiftParams p)
 {
     Ctrl *c = p.ctrl;
     T *F = (T *)p.F;
@@ -475,12 +727,16 @@ __global__ void __launch_bounds__(LIFT_BLOCK, 2) k_lift(const __grid_constant__ 
         uint32_t *nxt = (round & 1) ? p.B0 : p.B1;
         int *ctr = c->ctr[round & 1];
         cnt.any_new = 0;
+        unsigned long long t0 = 0, t1 = 0, t2 = 0;
+        if (p.profile) t0 = globaltimer_ns();
         if (p.num_tasks) heavy_tasks<T>(p, F, cur, nxt, cnt);
+        if (p.profile) t1 = globaltimer_ns();
         for (int ci = 0; ci < p.nclasses; ci++) {
             const LiftClass &lc = p.cls[ci];
-            if (lc.owner) run_class<T, 1>(p, lc, F, cur, nxt, ctr + ci, cnt);
-            else run_class<T, 0>(p, lc, F, cur, nxt, ctr + ci, cnt);
+            if (lc.owner) run_class<T, 1, LEAN>(p, lc, F, cur, nxt, ctr + ci, cnt);
+            else run_class<T, 0, LEAN>(p, lc, F, cur, nxt, ctr + ci, cnt);
         }
+        if (p.profile) t2 = globaltimer_ns();
         if (__syncthreads_or(cnt.any_new) && threadIdx.x == 0) c->flag[(round + 1) & 1] = 1;
         const bool ok = grid_barrier(c, p.wait_limit_ns, [&]() {
             /* last arriver of round `round`: clear this parity's counters
@@ -498,6 +754,12 @@ __global__ void __launch_bounds__(LIFT_BLOCK, 2) k_lift(const __grid_constant__ 
                 }
             }
         });
+        if (p.profile && (threadIdx.x & 31) == 0) {
+            const unsigned long long t3 = globaltimer_ns();
+            atomicAdd(&c->t_heavy, t1 - t0);
+            atomicAdd(&c->t_light, t2 - t1);
+            atomicAdd(&c->t_wait, t3 - t2);
+        }
         if (!ok) break;
         if (ld_volatile(&c->stop)) break;
         if (!ld_volatile(&c->flag[(round + 1) & 1])) break;
@@ -527,9 +789,9 @@ __device__ __forceinline__ void cta_warp_class(const LiftParams &p, const LiftCl
                                                const CtaPolicy &pol, int *ctr, LiftCounters &cnt)
 {
     const int lane = threadIdx.x & 31;
-    constexpr int NG = 32 / G;
+    constexpr int NG = G >= 32 ? 1 : 32 / G;
     const int grp = lane / G, gl = lane % G;
-    const unsigned gmask = (G == 32) ? 0xffffffffu : (((1u << G) - 1u) << (grp * G));
+    const unsigned gmask = (G >= 32) ? 0xffffffffu : (((1u << (G & 31)) - 1u) << (grp * G));
     const int nwords = lc.word_end - lc.word_begin;
     for (;;) {
         int wi = 0;
@@ -541,6 +803,10 @@ __device__ __forceinline__ void cta_warp_class(const LiftParams &p, const LiftCl
         __syncwarp();
         if (lane == 0 && word) cur[gw] = 0;
         const int base_u = gw << 5;
+        if (G == EG_GROUP_LIGHT) {
+            if (word) light_word<T, OWNER>(p, F, pol, gw, word, lane, cnt);
+            continue;
+        }
         if (G == 1) {
             if ((word >> lane) & 1u) lift_group<T, 1, OWNER>(p, F, pol, base_u + lane, 0, 0u, cnt);
             continue;
@@ -589,11 +855,13 @@ __global__ void __launch_bounds__(1024, 1) k_lift_cta(const __grid_constant__ Li
             int *ctr = &s_ctr[round & 1][ci];
             const int g = lc.group;
             if (lc.owner) {
-                if (g == 1) cta_warp_class<T, 1, 1>(p, lc, F, cur, pol, ctr, cnt);
+                if (g == EG_GROUP_LIGHT) cta_warp_class<T, EG_GROUP_LIGHT, 1>(p, lc, F, cur, pol, ctr, cnt);
+                else if (g == 1) cta_warp_class<T, 1, 1>(p, lc, F, cur, pol, ctr, cnt);
                 else if (g == 8) cta_warp_class<T, 8, 1>(p, lc, F, cur, pol, ctr, cnt);
                 else cta_warp_class<T, 32, 1>(p, lc, F, cur, pol, ctr, cnt);
             } else {
-                if (g == 1) cta_warp_class<T, 1, 0>(p, lc, F, cur, pol, ctr, cnt);
+                if (g == EG_GROUP_LIGHT) cta_warp_class<T, EG_GROUP_LIGHT, 0>(p, lc, F, cur, pol, ctr, cnt);
+                else if (g == 1) cta_warp_class<T, 1, 0>(p, lc, F, cur, pol, ctr, cnt);
                 else if (g == 8) cta_warp_class<T, 8, 0>(p, lc, F, cur, pol, ctr, cnt);
                 else cta_warp_class<T, 32, 0>(p, lc, F, cur, pol, ctr, cnt);
             }
@@ -656,7 +924,8 @@ eg_status launch_lift(const LiftParams &p, int credit_bits, cudaStream_t st, int
     cudaGetDevice(&dev);
     int sms = 0;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    const void *fn = credit_bits == 32 ? (const void *)k_lift<int32_t> : (const void *)k_lift<int64_t>;
+    const void *fn = credit_bits == 32 ? (p.lean ? (const void *)k_lift<int32_t, true> : (const void *)k_lift<int32_t, false>)
+                                       : (p.lean ? (const void *)k_lift<int64_t, true> : (const void *)k_lift<int64_t, false>);
     int per_sm = 0;
     cudaError_t err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, LIFT_BLOCK, 0);
     if (err != cudaSuccess || per_sm < 1)

@@ -10,7 +10,7 @@ namespace eg {
 
 /* Lane-group sizes of the lifting variants; EG_GROUP_CTA lifts one vertex
  * with the whole CTA. */
-enum { EG_GROUP_CTA = 0 };
+enum { EG_GROUP_CTA = 0, EG_GROUP_LIGHT = 64 };
 
 struct LiftClass {
     int word_begin, word_end;  /* frontier words of the class              */
@@ -41,6 +41,16 @@ struct LiftParams {
     int heavy_begin;
     void *hacc;                /* per heavy vertex: partial min / max (credit type) */
     int *hrem;                 /* per heavy vertex: tasks still to report          */
+    int profile;               /* non-zero: accumulate the phase timers of Ctrl    */
+    int lean;                  /* AUTO layout: use the lean kernel instantiation   */
+    /* direction switching (lean kernel): a round is dense (every vertex
+     * lifted, no frontier) after >= dense_min_changes raises, and goes back to
+     * the frontier below sparse_max_changes raises */
+    uint32_t *CH0, *CH1;       /* raised-in-round bitmaps, by parity               */
+    long long dense_min_changes, sparse_max_changes;
+    int direction;             /* 0 switch, 1 sparse only, 2 dense only           */
+    int light_word_end;        /* words [0, light_word_end) are light             */
+    int words;                 /* frontier words                                  */
 };
 
 /* Edge pairs per heavy task (256 edges). */

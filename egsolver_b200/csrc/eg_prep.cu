@@ -354,6 +354,25 @@ __global__ void k_init_frontier(int n_pad, const int *perm, const unsigned char 
     }
 }
 
+/* Predecessor lists padded to a multiple of 4 entries (pad = -1), so that
+ * a push reads four predecessors per 128-bit load. */
+__global__ void k_round4(int len, const int *in, int *out)
+{
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < len; i += (long long)gridDim.x * blockDim.x)
+        out[i] = (in[i] + 3) & ~3;
+}
+
+__global__ void k_csc_pad(int n_pad, const int *dense_off, const int *pad_off, const int *dense, int *padded)
+{
+    const int lane = threadIdx.x & 31;
+    const long long w0 = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const long long nw = ((long long)gridDim.x * blockDim.x) >> 5;
+    for (long long u = w0; u < n_pad; u += nw) {
+        const int db = dense_off[u], de = dense_off[u + 1], pb = pad_off[u], pe = pad_off[u + 1];
+        for (int k = lane; k < pe - pb; k += 32) padded[pb + k] = (db + k < de) ? dense[db + k] : -1;
+    }
+}
+
 /* ------------------------------------------------------------------ */
 /* Heavy vertices cut into edge tasks                                   */
 /* ------------------------------------------------------------------ */

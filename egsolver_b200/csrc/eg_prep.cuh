@@ -48,6 +48,8 @@ __global__ void k_copy_edges(int n_pad, const int *perm, const int *iperm, const
                              const int *w, const int *P, int2 *E, int *csc_key, int *csc_val, int *indeg,
                              ClassTable ct, int topv, int zerov);
 __global__ void k_init_frontier(int n_pad, const int *perm, const unsigned char *active0, uint32_t *B);
+__global__ void k_round4(int len, const int *in, int *out);
+__global__ void k_csc_pad(int n_pad, const int *dense_off, const int *pad_off, const int *dense, int *padded);
 /* heavy tasks: per heavy vertex the number of 256-edge tasks, then the tasks */
 __global__ void k_task_count(int heavy_begin, int n_pad, const int *P, int task_pairs, int *count);
 __global__ void k_task_fill(int heavy_begin, int n_pad, const int *P, int task_pairs, const int *toff, ClassTable ct,

@@ -101,7 +101,12 @@ typedef struct eg_opts {
                                     previous solve of the same resident game           */
     int32_t grid_ctas;           /* cap on the lifting grid's CTAs (0: every SM, full
                                     occupancy); a smaller grid leaves SMs to other work */
-    int32_t reserved[4];
+    int32_t task_edges;          /* edges per task of a heavy vertex, 32..256 (0: 256) */
+    int32_t schedule;            /* light words: 0 dealt evenly to warps, 1 taken in
+                                    increasing order from a counter                   */
+    int32_t profile;             /* non-zero: report the kernel's phase timers        */
+    int32_t ctas_per_sm;         /* AUTO layout: 3 = lean kernel at three CTAs per SM,
+                                    2 = full kernel at two (0: 3)                     */
 } eg_opts;
 
 typedef struct eg_stats {
@@ -120,6 +125,9 @@ typedef struct eg_stats {
     int64_t pushes;              /* predecessor entries scanned after those raises    */
     int32_t grid, block;         /* launch shape of the lifting kernel                */
     int32_t reserved[2];
+    /* with opts.profile: mean time per warp and round in heavy tasks, in word
+     * classes, and waiting at the round barrier (nanoseconds) */
+    double  phase_heavy_ns, phase_light_ns, phase_wait_ns;
 } eg_stats;
 
 /* ------------------------------------------------------------------ */
