@@ -18,8 +18,8 @@ from typing import Optional
 import numpy as np
 
 from . import _ffi
-from ._ffi import (EG_TOP32, EG_TOP64, VARIANT_AUTO, VARIANT_CTA, VARIANT_SMEM, VARIANT_THREAD,  # noqa: F401
-                   VARIANT_WARP)
+from ._ffi import (DIRECTION_DENSE, DIRECTION_SPARSE, DIRECTION_SWITCH, EG_TOP32, EG_TOP64,  # noqa: F401
+                   VARIANT_AUTO, VARIANT_CTA, VARIANT_SMEM, VARIANT_THREAD, VARIANT_WARP)
 
 __all__ = ["Game", "EGError", "Stats", "solve", "ResidentGame", "Batch", "BatchStats", "Server", "threshold_game",
            "generate", "read_game", "read_game_text",
@@ -122,6 +122,7 @@ class Stats:
     pushes: int
     grid: int
     block: int
+    dense_rounds: int
     phase_heavy_ns: float
     phase_light_ns: float
     phase_wait_ns: float
@@ -138,7 +139,8 @@ class Stats:
 def make_opts(credit_bits: int = 64, variant: int = VARIANT_AUTO, max_rounds: int = -1, timeout_ms: float = 0.0,
               device: int = 0, lanes_per_vertex: int = 0, small_max_deg: int = 0, large_min_deg: int = 0,
               keep_layout: bool = False, cancel: Optional["CancelFlag"] = None, grid_ctas: int = 0,
-              task_edges: int = 0, schedule: int = 0, profile: bool = False, ctas_per_sm: int = 0) -> _ffi.EgOpts:
+              task_edges: int = 0, schedule: int = 0, profile: bool = False, ctas_per_sm: int = 0,
+              direction: int = 0, dense_permille: int = 0, sparse_permille: int = 0) -> _ffi.EgOpts:
     o = _ffi.EgOpts()
     lib().eg_opts_default(C.byref(o))
     o.credit_bits = credit_bits
@@ -155,6 +157,9 @@ def make_opts(credit_bits: int = 64, variant: int = VARIANT_AUTO, max_rounds: in
     o.schedule = schedule
     o.profile = 1 if profile else 0
     o.ctas_per_sm = ctas_per_sm
+    o.direction = direction
+    o.dense_permille = dense_permille
+    o.sparse_permille = sparse_permille
     o.cancel = cancel.ptr if cancel is not None else None
     return o
 

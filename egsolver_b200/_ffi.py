@@ -21,6 +21,7 @@ EG_TOP32 = 2147483647
 EG_TOP64 = 9223372036854775807
 
 VARIANT_AUTO, VARIANT_THREAD, VARIANT_WARP, VARIANT_CTA, VARIANT_SMEM = 0, 1, 2, 3, 4
+DIRECTION_SWITCH, DIRECTION_SPARSE, DIRECTION_DENSE = 0, 1, 2
 
 
 class EgGame(C.Structure):
@@ -52,6 +53,9 @@ class EgOpts(C.Structure):
         ("schedule", C.c_int32),
         ("profile", C.c_int32),
         ("ctas_per_sm", C.c_int32),
+        ("direction", C.c_int32),
+        ("dense_permille", C.c_int32),
+        ("sparse_permille", C.c_int32),
     ]
 
 
@@ -75,7 +79,8 @@ class EgStats(C.Structure):
         ("pushes", C.c_int64),
         ("grid", C.c_int32),
         ("block", C.c_int32),
-        ("reserved", C.c_int32 * 2),
+        ("dense_rounds", C.c_int32),
+        ("reserved", C.c_int32),
         ("phase_heavy_ns", C.c_double),
         ("phase_light_ns", C.c_double),
         ("phase_wait_ns", C.c_double),

@@ -34,7 +34,7 @@ CC_FLAGS = ["-O3", "-fPIC", "-std=gnu11", "-Wall", "-Wno-unused-function", "-I",
             "-I", str(CUDA_HOME / "include")]
 
 C_SOURCES = ["eg_host.c", "eg_reader.c"]
-CU_SOURCES = ["eg_prep.cu", "eg_lift.cu", "eg_api.cu", "eg_batch.cu", "eg_serve.cu", "eg_noalloc.cu"]
+CU_SOURCES = ["eg_prep.cu", "eg_lift.cu", "eg_dense.cu", "eg_api.cu", "eg_batch.cu", "eg_serve.cu", "eg_noalloc.cu"]
 REFABI_SOURCES = ["eg_refabi.c"]
 
 

@@ -41,6 +41,9 @@ constexpr int kPrepBlock = 256;
 /* AUTO lifts a game with one CTA (frontier in shared memory) up to this
  * many edges; larger games use the persistent grid. */
 constexpr long long kSmallGameEdges = 1 << 17;
+/* default round-kind thresholds, raises per thousand vertices */
+constexpr long long kDensePermille = 40;
+constexpr long long kSparsePermille = 15;
 constexpr int kSmallGameMaxPad = 1 << 19;
 
 inline unsigned grid_for(long long items, int block, int cap = 148 * 32)
@@ -91,6 +94,12 @@ struct eg_dgame {
     int *d_hrem, *d_toff;
     long long task_cap;
     int num_tasks, heavy_begin, heavy_bucket, task_pairs;
+    /* dense rounds: pair-stream metadata and cut-vertex accumulators */
+    uint16_t *d_PM;
+    int *d_CB, *d_merr, *d_drem;
+    void *d_dacc;
+    int npairs;
+    bool meta_ok;
     size_t bytes;
     long long mg;
     int solved_bits;
@@ -183,6 +192,10 @@ static eg_status check_lanes(const eg_opts *o)
         return eg_set_error(EG_ERR_INVALID, "unknown variant %d", o->variant);
     if (o && o->credit_bits != 0 && o->credit_bits != 32 && o->credit_bits != 64)
         return eg_set_error(EG_ERR_INVALID, "credit_bits must be 32 or 64 (got %d)", o->credit_bits);
+    if (o && (o->direction < EG_DIRECTION_SWITCH || o->direction > EG_DIRECTION_DENSE))
+        return eg_set_error(EG_ERR_INVALID, "unknown direction %d", o->direction);
+    if (o && (o->dense_permille < 0 || o->dense_permille > 1000 || o->sparse_permille < 0 || o->sparse_permille > 1000))
+        return eg_set_error(EG_ERR_INVALID, "round-kind thresholds must be 0..1000 per mille");
     return EG_OK;
 }
 
@@ -215,7 +228,7 @@ extern "C" void eg_dgame_free(eg_dgame *g)
     void *ptrs[] = {g->d_rowptr, g->d_succ, g->d_w, g->d_owner, g->d_perm, g->d_iperm, g->d_P, g->d_CP,
                     g->d_CS, g->d_E, g->d_active0, g->d_k0, g->d_v0, g->d_k1, g->d_v1, g->d_scratch,
                     g->d_counts, g->d_mg, g->d_F, g->d_out, g->d_B, g->d_ctrl, g->d_tasks, g->d_hacc,
-                    g->d_hrem, g->d_toff};
+                    g->d_hrem, g->d_toff, g->d_PM, g->d_CB, g->d_merr, g->d_drem, g->d_dacc};
     for (void *p : ptrs)
         if (p) cudaFree(p);
     for (int i = 0; i < 4; i++)
@@ -275,13 +288,18 @@ static eg_status dgame_alloc(const eg_game *game, const eg_opts *opts, eg_dgame 
     if (s == EG_OK) s = dalloc(g, &g->d_mg, 1);
     if (s == EG_OK) s = dalloc(g, (int64_t **)&g->d_F, (size_t)g->n_pad_cap + 64);
     if (s == EG_OK) s = dalloc(g, (int64_t **)&g->d_out, (size_t)g->n);
-    if (s == EG_OK) s = dalloc(g, &g->d_B, (size_t)(2 * words));
+    if (s == EG_OK) s = dalloc(g, &g->d_B, (size_t)(4 * words)); /* two frontiers, two raised-maps */
     if (s == EG_OK) s = dalloc(g, &g->d_ctrl, 1);
     g->task_cap = g->m_pad_cap / 32 + g->n_pad_cap + 2; /* tasks of >= 16 pairs */
     if (s == EG_OK) s = dalloc(g, &g->d_tasks, (size_t)g->task_cap);
     if (s == EG_OK) s = dalloc(g, (int64_t **)&g->d_hacc, (size_t)g->n_pad_cap);
     if (s == EG_OK) s = dalloc(g, &g->d_hrem, (size_t)g->n_pad_cap);
     if (s == EG_OK) s = dalloc(g, &g->d_toff, (size_t)g->n_pad_cap + 1);
+    if (s == EG_OK) s = dalloc(g, &g->d_PM, (size_t)(g->m_pad_cap / 2 + 64));
+    if (s == EG_OK) s = dalloc(g, &g->d_CB, (size_t)(g->m_pad_cap / 64 + 4));
+    if (s == EG_OK) s = dalloc(g, &g->d_merr, 1);
+    if (s == EG_OK) s = dalloc(g, &g->d_drem, (size_t)g->n_pad_cap);
+    if (s == EG_OK) s = dalloc(g, (int64_t **)&g->d_dacc, (size_t)g->n_pad_cap);
     if (s != EG_OK) {
         eg_dgame_free(g);
         return s;
@@ -433,6 +451,21 @@ static eg_status dgame_prepare(eg_dgame *g, const eg_opts *opts)
             }
         }
     }
+    /* AUTO layout: the pair stream of the dense rounds */
+    g->meta_ok = false;
+    g->npairs = 0;
+    if (!opts || opts->variant == EG_VARIANT_AUTO || opts->variant == EG_VARIANT_SMEM) {
+        int pend = 0, merr = 0;
+        EG_CUDA(cudaMemsetAsync(g->d_merr, 0, sizeof(int), st));
+        EG_CUDA(cudaMemcpyAsync(&pend, g->d_P + n_pad, sizeof pend, cudaMemcpyDeviceToHost, st));
+        EG_CUDA(cudaStreamSynchronize(st));
+        g->npairs = pend / 2;
+        build_pair_meta(g->d_P, n_pad, g->npairs, g->ct, g->d_PM, g->d_CB, g->d_merr, st);
+        EG_CUDA(cudaMemcpyAsync(&merr, g->d_merr, sizeof merr, cudaMemcpyDeviceToHost, st));
+        EG_CUDA(cudaStreamSynchronize(st));
+        g->meta_ok = merr == 0 && g->npairs > 0;
+        g->launches += 2;
+    }
     EG_CUDA(cudaGetLastError());
     g->prepared = true;
     return EG_OK;
@@ -458,7 +491,7 @@ extern "C" eg_status eg_dgame_solve(eg_dgame *g, const eg_opts *opts_in, eg_stat
     const int topv = n_pad;
     launch_init_credits(bits, n_pad + 64, g->d_F, topv, st);
     const long long wds = g->words + 2;
-    EG_CUDA(cudaMemsetAsync(g->d_B, 0, sizeof(uint32_t) * (size_t)(2 * wds), st));
+    EG_CUDA(cudaMemsetAsync(g->d_B, 0, sizeof(uint32_t) * (size_t)(4 * wds), st));
     k_init_frontier<<<grid_for(n_pad, kPrepBlock), kPrepBlock, 0, st>>>(n_pad, g->d_perm, g->d_active0, g->d_B);
     EG_CUDA(cudaMemsetAsync(g->d_ctrl, 0, sizeof(Ctrl), st));
     g->launches += 2;
@@ -472,6 +505,8 @@ extern "C" eg_status eg_dgame_solve(eg_dgame *g, const eg_opts *opts_in, eg_stat
     p.F = g->d_F;
     p.B0 = g->d_B;
     p.B1 = g->d_B + wds;
+    p.CH0 = g->d_B + 2 * wds;
+    p.CH1 = g->d_B + 3 * wds;
     p.ctrl = g->d_ctrl;
     p.mg = g->mg;
     p.max_rounds = opts->max_rounds;
@@ -507,6 +542,16 @@ extern "C" eg_status eg_dgame_solve(eg_dgame *g, const eg_opts *opts_in, eg_stat
     p.nclasses = nc;
     p.lean = tasks && (opts->variant == EG_VARIANT_AUTO || opts->variant == EG_VARIANT_SMEM) && opts->ctas_per_sm != 2 &&
              opts->small_max_deg <= 0; /* the lean kernel knows only light words and tasks */
+    /* round kinds: the lean layout alternates frontier rounds (k_lift) and
+     * dense rounds (k_lift_dense) */
+    const bool kinds = p.lean && g->meta_ok && opts->direction != EG_DIRECTION_SPARSE;
+    p.direction = kinds ? opts->direction : EG_DIRECTION_SPARSE;
+    {
+        const long long dpm = opts->dense_permille > 0 ? opts->dense_permille : kDensePermille;
+        const long long spm = opts->sparse_permille > 0 ? opts->sparse_permille : kSparsePermille;
+        p.dense_min_changes = std::max(1LL, (dpm * g->n + 999) / 1000);
+        p.sparse_max_changes = spm * g->n / 1000;
+    }
     if (tasks) {
         launch_task_reset(bits, g->heavy_begin, n_pad, g->d_toff, g->ct, g->d_hacc, g->d_hrem, st);
         g->launches++;
@@ -516,16 +561,51 @@ extern "C" eg_status eg_dgame_solve(eg_dgame *g, const eg_opts *opts_in, eg_stat
         p.hacc = g->d_hacc;
         p.hrem = g->d_hrem;
     }
-    int grid = 0, block = 0;
+    int grid = 0, block = 0, dgrid = 0;
+    if (kinds) {
+        /* one slice of the pair stream per warp of the dense grid */
+        EG_TRY(dense_grid(bits, opts->grid_ctas, &dgrid));
+        const long long warps = (long long)dgrid * 16;
+        const long long per = (g->npairs + warps - 1) / warps;
+        p.PM = g->d_PM;
+        p.CB = g->d_CB;
+        p.npairs = g->npairs;
+        p.slice = (int)std::max(32LL, (per + 31) / 32 * 32);
+        p.dacc = g->d_dacc;
+        p.drem = g->d_drem;
+        launch_dense_setup(p, bits, st);
+        g->launches++;
+    }
     EG_CUDA(cudaEventRecord(g->ev[1], st));
     if (small) {
         EG_TRY(launch_lift_cta(p, bits, st));
         grid = 1;
         block = 1024;
-    } else {
+        g->launches++;
+    } else if (!kinds) {
         EG_TRY(launch_lift(p, bits, st, &grid, &block, opts->grid_ctas));
+        g->launches++;
+    } else {
+        /* frontier and dense kernels take turns; each returns when its last
+         * round picks the other kind (or the solve ends) */
+        int kind = opts->direction == EG_DIRECTION_DENSE ? ROUND_DENSE : ROUND_SPARSE;
+        for (;;) {
+            if (kind == ROUND_DENSE) {
+                EG_TRY(launch_lift_dense(p, bits, st, dgrid));
+                grid = dgrid;
+                block = 512;
+            } else {
+                EG_TRY(launch_lift(p, bits, st, &grid, &block, opts->grid_ctas));
+            }
+            g->launches++;
+            int tail[2] = {0, 0}; /* stop, next_mode */
+            EG_CUDA(cudaMemcpyAsync(&tail[0], &g->d_ctrl->stop, sizeof(int), cudaMemcpyDeviceToHost, st));
+            EG_CUDA(cudaMemcpyAsync(&tail[1], &g->d_ctrl->next_mode, sizeof(int), cudaMemcpyDeviceToHost, st));
+            EG_CUDA(cudaStreamSynchronize(st));
+            if (tail[0] || tail[1] == ROUND_DONE) break;
+            kind = (tail[1] == ROUND_DENSE || tail[1] == ROUND_RECORD) ? ROUND_DENSE : ROUND_SPARSE;
+        }
     }
-    g->launches++;
     EG_CUDA(cudaEventRecord(g->ev[2], st));
     launch_count_top(bits, n_pad, g->d_F, &g->d_ctrl->num_top, st);
     g->launches++;
@@ -558,6 +638,7 @@ extern "C" eg_status eg_dgame_solve(eg_dgame *g, const eg_opts *opts_in, eg_stat
         stats->pushes = (int64_t)ctrl.pushes;
         stats->grid = grid;
         stats->block = block;
+        stats->dense_rounds = (int32_t)ctrl.dense_rounds;
         if (p.profile) {
             /* average per warp and round, in nanoseconds */
             const double wr = (double)grid * (block / 32) * (double)(ctrl.rounds ? ctrl.rounds : 1);

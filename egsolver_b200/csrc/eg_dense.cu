@@ -1,0 +1,398 @@
+/*
+ * eg_dense.cu -- dense rounds: every vertex lifted, no frontier.
+ *
+ * When a large share of the credits rise in each round (the usual case on
+ * large random games, where most vertices have a raised successor every
+ * round), a frontier round spends most of its time pushing predecessors
+ * into a bitmap that ends up nearly full.  A dense round lifts every vertex
+ * against the current credits instead and pushes nothing: it reads the
+ * edge pairs once, in order, and gathers the successors' credits.
+ *
+ * The padded edge-pair array E4 (pairs of one vertex are contiguous, see
+ * k_copy_edges) is one stream of `npairs` pairs.  It is cut into equal
+ * slices of `slice` pairs (a multiple of 32), one per warp of the grid, so
+ * the work is balanced by construction whatever the degree distribution.
+ * A warp walks its slice 32 pairs (one chunk) at a time: lane j gathers the
+ * two successor credits of pair j and applies OMINUS, and a segmented
+ * shuffle scan over runs of equal vertex gives every vertex's min (player 0)
+ * or max (player 1) -- the max is taken as a min of negated values so one
+ * scan serves both owners.  A vertex that runs on into the next chunk
+ * carries its partial value in registers; a vertex cut by a slice edge
+ * combines the partial values of all its slices with an atomic min / max,
+ * and the slice that reports last finalizes it (reporter counts from
+ * k_dense_setup).  Per pair, 16 bits of metadata (PM) give the owner, "last
+ * pair of its vertex" and the vertex as an offset from the chunk's first
+ * vertex (CB).
+ *
+ * Exactness: each dense round lifts every vertex once against credits that
+ * are the round's start values or values raised during the round, all
+ * below the least fixed point; a round without a raise has lifted every
+ * vertex against the final credits, so they are the least fixed point.  This
+ * is the same fair chaotic iteration as the reference's worklist loop
+ * (reference src/dev_EG_alg.cu:307-381), so the credits are bit-identical.
+ *
+ * Hand-over to frontier rounds (k_lift): when a dense round raises fewer
+ * than sparse_max_changes credits, the next round records its raised
+ * vertices in the bitmap CH[r&1] (a "recording" round); if it too stays
+ * below the bound, the kernel returns with Ctrl::next_mode = ROUND_SEED and
+ * k_lift starts by pushing the predecessors of the recorded vertices.  Every
+ * dense round clears CH[(r+1)&1], so a recording round always starts from a
+ * clear map.
+ */
+#include "eg_lift.cuh"
+#include "eg_prep.cuh"
+
+namespace eg {
+
+constexpr int DENSE_BLOCK = 512;
+constexpr int kMetaBlock = 256;
+constexpr uint32_t PM_OWNER = 0x8000u, PM_END = 0x4000u, PM_OFF = 0x3fffu;
+
+template <class T>
+__device__ __forceinline__ T shfl_up_t(T v, int off)
+{
+    return __shfl_up_sync(0xffffffffu, v, off);
+}
+template <>
+__device__ __forceinline__ int64_t shfl_up_t<int64_t>(int64_t v, int off)
+{
+    return (int64_t)__shfl_up_sync(0xffffffffu, (long long)v, off);
+}
+template <class T>
+__device__ __forceinline__ T shfl_t(T v, int src)
+{
+    return __shfl_sync(0xffffffffu, v, src);
+}
+template <>
+__device__ __forceinline__ int64_t shfl_t<int64_t>(int64_t v, int src)
+{
+    return (int64_t)__shfl_sync(0xffffffffu, (long long)v, src);
+}
+
+/* ------------------------------------------------------------------ */
+/* Pair-stream metadata (once per layout)                               */
+/* ------------------------------------------------------------------ */
+
+/* The vertex whose pairs hold pair t: the largest u with P[u] / 2 <= t.
+ * Padding slots own no pairs and share the next vertex's offset, so they
+ * are never the largest such u. */
+__device__ __forceinline__ int pair_vertex(const int *P, int n_pad, int t)
+{
+    int lo = 0, hi = n_pad; /* P[lo] / 2 <= t < P[hi] / 2 */
+    while (hi - lo > 1) {
+        const int mid = lo + ((hi - lo) >> 1);
+        if ((__ldg(P + mid) >> 1) <= t) lo = mid;
+        else hi = mid;
+    }
+    return lo;
+}
+
+__global__ void k_chunk_base(const int *P, int n_pad, int npairs, int *CB)
+{
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if ((long long)c * 32 >= npairs) return;
+    CB[c] = pair_vertex(P, n_pad, c * 32);
+}
+
+__global__ void k_pair_meta(const int *P, int n_pad, int npairs, const ClassTable ct, const int *CB, uint16_t *PM,
+                            int *err)
+{
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= npairs) return;
+    const int u = pair_vertex(P, n_pad, t);
+    int off = u - CB[t >> 5];
+    if (off < 0 || off > (int)PM_OFF) {
+        atomicExch(err, 1);
+        off = 0;
+    }
+    const bool end = t == (__ldg(P + u + 1) >> 1) - 1;
+    PM[t] = (uint16_t)((ct.owner_of_new(u) ? PM_OWNER : 0u) | (end ? PM_END : 0u) | (uint32_t)off);
+}
+
+void build_pair_meta(const int *P, int n_pad, int npairs, const ClassTable &ct, uint16_t *PM, int *CB, int *err,
+                     cudaStream_t st)
+{
+    if (npairs <= 0) return;
+    const int nchunks = (npairs + 31) / 32;
+    k_chunk_base<<<(nchunks + kMetaBlock - 1) / kMetaBlock, kMetaBlock, 0, st>>>(P, n_pad, npairs, CB);
+    k_pair_meta<<<(npairs + kMetaBlock - 1) / kMetaBlock, kMetaBlock, 0, st>>>(P, n_pad, npairs, ct, CB, PM, err);
+}
+
+/* ------------------------------------------------------------------ */
+/* Per solve: reporter counts of the vertices cut by slice edges         */
+/* ------------------------------------------------------------------ */
+
+template <class T>
+__global__ void k_dense_setup(const int *P, int n_pad, const uint16_t *PM, int slice, T *dacc, int *drem)
+{
+    const int u = blockIdx.x * blockDim.x + threadIdx.x;
+    if (u >= n_pad) return;
+    const int b = P[u] >> 1, e = P[u + 1] >> 1;
+    if (e <= b) return;
+    const int nrep = (e - 1) / slice - b / slice + 1;
+    if (nrep > 1) {
+        drem[u] = nrep;
+        dacc[u] = (PM[b] & PM_OWNER) ? (T)0 : credit_traits<T>::top;
+    }
+}
+
+void launch_dense_setup(const LiftParams &p, int credit_bits, cudaStream_t st)
+{
+    const int grid = (p.n_pad + kMetaBlock - 1) / kMetaBlock;
+    if (credit_bits == 32)
+        k_dense_setup<int32_t><<<grid, kMetaBlock, 0, st>>>(p.P, p.n_pad, p.PM, p.slice, (int32_t *)p.dacc, p.drem);
+    else
+        k_dense_setup<int64_t><<<grid, kMetaBlock, 0, st>>>(p.P, p.n_pad, p.PM, p.slice, (int64_t *)p.dacc, p.drem);
+}
+
+/* ------------------------------------------------------------------ */
+/* The dense-round kernel                                               */
+/* ------------------------------------------------------------------ */
+
+struct DenseCounters {
+    unsigned long long lifts, edges;
+    unsigned changes;
+};
+
+/* A slice's partial value v (actual, not negated) of cut vertex u; the
+ * slice that reports last raises the credit.  Returns whether it rose. */
+template <class T>
+__device__ __forceinline__ bool dense_report(const LiftParams &p, T *F, int u, bool own, T v, DenseCounters &cnt)
+{
+    T *acc = (T *)p.dacc;
+    if (own) atomic_combine<1>(acc + u, v);
+    else atomic_combine<0>(acc + u, v);
+    __threadfence();
+    if (atomicSub(p.drem + u, 1) != 1) return false;
+    __threadfence();
+    const T r = atomic_swap(acc + u, own ? (T)0 : credit_traits<T>::top);
+    const int b = __ldg(p.P + u) >> 1, e = __ldg(p.P + u + 1) >> 1;
+    p.drem[u] = (e - 1) / p.slice - b / p.slice + 1; /* ready for the next round */
+    cnt.lifts++;
+    const T old = ld_credit(F + u);
+    if (old < r) {
+        st_credit(F + u, r);
+        cnt.changes++;
+        return true;
+    }
+    return false;
+}
+
+/* Recording round: OR the raised vertices of this chunk into `ch`, one
+ * atomic per distinct word (the raised vertices' ids rise with the lane). */
+__device__ __forceinline__ void mark_raised(uint32_t *ch, int u, bool raise, int lane)
+{
+    unsigned rm = __ballot_sync(0xffffffffu, raise);
+    while (rm) {
+        const int l = __ffs(rm) - 1;
+        const int wd = __shfl_sync(0xffffffffu, u >> 5, l);
+        const bool mine = raise && (u >> 5) == wd;
+        const unsigned same = __ballot_sync(0xffffffffu, mine);
+        const uint32_t bits = __reduce_or_sync(0xffffffffu, mine ? (1u << (u & 31)) : 0u);
+        if (lane == l) atomicOr(ch + wd, bits);
+        rm &= ~same;
+    }
+}
+
+/* One warp's slice [s0, s1) of the pair stream. */
+template <class T>
+__device__ __forceinline__ void dense_slice(const LiftParams &p, T *F, uint32_t *ch, bool rec, int s0, int s1,
+                                            int lane, DenseCounters &cnt)
+{
+    constexpr T top = credit_traits<T>::top;
+    if (s0 >= s1) return;
+    const uint32_t le_mask = 0xffffffffu >> (31 - lane);
+    /* the vertex of the slice's first pair began in an earlier slice? */
+    bool carry_on = s0 > 0 && !(__ldg(p.PM + s0 - 1) & PM_END);
+    bool carry_cut = carry_on;
+    T carry = top; /* min-space partial of the carried vertex */
+    int carry_u = 0;
+    bool carry_own = false;
+    /* chunk 0, then each iteration loads the next chunk before it works */
+    int t = s0 + lane;
+    bool in = t < s1;
+    int4 q = make_int4(0, 0, 0, 0);
+    uint32_t md = PM_END;
+    if (in) {
+        q = __ldg(p.E4 + t);
+        md = __ldg(p.PM + t);
+    }
+    int base = __ldg(p.CB + (s0 >> 5));
+    for (int c0 = s0; c0 < s1; c0 += 32) {
+        const int tn = c0 + 32 + lane;
+        const bool inn = tn < s1;
+        int4 qn = make_int4(0, 0, 0, 0);
+        uint32_t mdn = PM_END;
+        int basen = 0;
+        if (inn) {
+            qn = __ldg(p.E4 + tn);
+            mdn = __ldg(p.PM + tn);
+        }
+        if (c0 + 32 < s1) basen = __ldg(p.CB + ((c0 + 32) >> 5));
+
+        const int u = base + (int)(md & PM_OFF);
+        const bool own = (md & PM_OWNER) != 0;
+        const bool end = (md & PM_END) != 0; /* lanes past the slice end count as ends */
+        T x = top, old = (T)0;
+        if (in) {
+            const T f0 = ld_credit(F + q.x), f1 = ld_credit(F + q.z);
+            if (end) old = ld_credit(F + u);
+            const T v0 = ominus<T>(f0, q.y, p.mg), v1 = ominus<T>(f1, q.w, p.mg);
+            x = own ? -(v0 > v1 ? v0 : v1) : (v0 < v1 ? v0 : v1);
+            cnt.edges += 1ull + (q.z < p.n_pad);
+        }
+        /* segmented inclusive min over runs of one vertex */
+        const uint32_t ends = __ballot_sync(0xffffffffu, end);
+        const int head = 31 - __clz(((ends << 1) | 1u) & le_mask);
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const T y = shfl_up_t<T>(x, o);
+            if (lane - o >= head && y < x) x = y;
+        }
+        if (carry_on && head == 0 && carry < x) x = carry;
+        /* vertices whose last pair is here */
+        bool raise = false;
+        if (in && end) {
+            const T v = own ? -x : x;
+            if (head == 0 && carry_cut) {
+                raise = dense_report<T>(p, F, u, own, v, cnt);
+            } else {
+                cnt.lifts++;
+                if (old < v) {
+                    st_credit(F + u, v);
+                    cnt.changes++;
+                    raise = true;
+                }
+            }
+        }
+        if (rec) mark_raised(ch, u, raise, lane);
+        /* the last lane's vertex runs on into the next chunk? */
+        const bool open = !(ends >> 31);
+        carry_cut = open && carry_cut && (ends & 0x7fffffffu) == 0u;
+        carry_on = open;
+        carry = shfl_t<T>(x, 31);
+        carry_u = __shfl_sync(0xffffffffu, u, 31);
+        carry_own = __shfl_sync(0xffffffffu, (int)own, 31) != 0;
+        q = qn;
+        md = mdn;
+        base = basen;
+        in = inn;
+    }
+    /* the last vertex goes on in the next slice: report its part */
+    if (carry_on && lane == 0) {
+        const bool r = dense_report<T>(p, F, carry_u, carry_own, carry_own ? -carry : carry, cnt);
+        if (rec && r) atomicOr(ch + (carry_u >> 5), 1u << (carry_u & 31));
+    }
+}
+
+/* Persistent dense rounds from round Ctrl::rounds until the last arriver
+ * picks another kind: ROUND_DONE (no raise: solved), or ROUND_SEED after a
+ * recording round below sparse_max_changes. */
+template <class T>
+__global__ void __launch_bounds__(DENSE_BLOCK, 3) k_lift_dense(const __grid_constant__ LiftParams p)
+{
+    __shared__ unsigned long long s_changes;
+    Ctrl *c = p.ctrl;
+    T *F = (T *)p.F;
+    DenseCounters cnt = {0ull, 0ull, 0u};
+    const int lane = threadIdx.x & 31;
+    const int gthr = (int)(blockIdx.x * blockDim.x + threadIdx.x);
+    const int nthr = (int)(gridDim.x * blockDim.x);
+    const long long sl = (long long)(gthr >> 5) * p.slice;
+    const int s0 = (int)(sl < p.npairs ? sl : p.npairs);
+    const int s1 = (int)(sl + p.slice < p.npairs ? sl + p.slice : p.npairs);
+    const int words = p.n_pad >> 5;
+    if (blockIdx.x == 0 && threadIdx.x == 0 && c->t_start == 0ull) c->t_start = globaltimer_ns();
+    if (threadIdx.x == 0) s_changes = 0ull;
+    __syncthreads();
+    const long long round0 = ld_volatile(&c->rounds);
+    for (long long round = round0;; round++) {
+        const int kind = round == round0 ? ROUND_DENSE : ld_volatile(&c->next_mode);
+        uint32_t *cur = (round & 1) ? p.B1 : p.B0;
+        uint32_t *ch = (round & 1) ? p.CH1 : p.CH0;
+        uint32_t *chn = (round & 1) ? p.CH0 : p.CH1;
+        /* the frontier left by frontier rounds is not used; the other
+         * raised-map must be clear for a recording round next */
+        for (int w = gthr; w < words; w += nthr) {
+            if (round == round0) __stcg(cur + w, 0u);
+            __stcg(chn + w, 0u);
+        }
+        const unsigned changes0 = cnt.changes;
+        dense_slice<T>(p, F, ch, kind == ROUND_RECORD, s0, s1, lane, cnt);
+        unsigned d = cnt.changes - changes0;
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) d += __shfl_xor_sync(0xffffffffu, d, off);
+        if (lane == 0 && d) atomicAdd(&s_changes, (unsigned long long)d);
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            if (s_changes) atomicAdd(&c->round_changes[round & 1], s_changes);
+            s_changes = 0ull;
+        }
+        const bool ok = grid_barrier(c, p.wait_limit_ns, [&]() {
+            c->flag[round & 1] = 0;
+            c->rounds = round + 1;
+            c->dense_rounds++;
+            const unsigned long long raised = c->round_changes[round & 1];
+            c->round_changes[(round + 1) & 1] = 0ull;
+            int next;
+            if (raised == 0ull) {
+                next = ROUND_DONE;
+            } else if (p.direction == EG_DIRECTION_DENSE || (long long)raised >= p.sparse_max_changes) {
+                next = ROUND_DENSE;
+            } else if (kind == ROUND_RECORD) {
+                next = ROUND_SEED;
+                c->flag[(round + 1) & 1] = 1;
+            } else {
+                next = ROUND_RECORD;
+            }
+            c->next_mode = next;
+            if (raised) check_stop(p, c, round);
+        });
+        if (!ok) break;
+        if (ld_volatile(&c->stop)) break;
+        const int nk = ld_volatile(&c->next_mode);
+        if (nk != ROUND_DENSE && nk != ROUND_RECORD) break;
+    }
+    unsigned long long l = cnt.lifts, e = cnt.edges, chg = cnt.changes;
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) {
+        l += __shfl_xor_sync(0xffffffffu, l, off);
+        e += __shfl_xor_sync(0xffffffffu, e, off);
+        chg += __shfl_xor_sync(0xffffffffu, chg, off);
+    }
+    if (lane == 0) {
+        atomicAdd(&c->lifts, l);
+        atomicAdd(&c->edges, e);
+        atomicAdd(&c->changes, chg);
+    }
+}
+
+static const void *dense_fn(int credit_bits)
+{
+    return credit_bits == 32 ? (const void *)k_lift_dense<int32_t> : (const void *)k_lift_dense<int64_t>;
+}
+
+eg_status dense_grid(int credit_bits, int max_ctas, int *grid)
+{
+    int dev = 0, sms = 0, per_sm = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaError_t err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, dense_fn(credit_bits), DENSE_BLOCK, 0);
+    if (err != cudaSuccess || per_sm < 1)
+        return eg_set_error(EG_ERR_CUDA, "occupancy query for the dense kernel failed: %s", cudaGetErrorString(err));
+    int g = sms * per_sm;
+    if (max_ctas > 0 && max_ctas < g) g = max_ctas;
+    *grid = g;
+    return EG_OK;
+}
+
+eg_status launch_lift_dense(const LiftParams &p, int credit_bits, cudaStream_t st, int grid)
+{
+    void *args[] = {(void *)&p};
+    cudaError_t err = cudaLaunchCooperativeKernel(dense_fn(credit_bits), dim3(grid), dim3(DENSE_BLOCK), args, 0, st);
+    if (err != cudaSuccess)
+        return eg_set_error(EG_ERR_CUDA, "cooperative launch of the dense kernel failed: %s", cudaGetErrorString(err));
+    return EG_OK;
+}
+
+}  // namespace eg

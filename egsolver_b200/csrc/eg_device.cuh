@@ -55,6 +55,7 @@ __device__ __forceinline__ void st_release_gpu(unsigned *p, unsigned v)
     asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
 }
 __device__ __forceinline__ int ld_volatile(const int *p) { return *(volatile const int *)p; }
+__device__ __forceinline__ long long ld_volatile(const long long *p) { return *(volatile const long long *)p; }
 
 /* Sets bit p of a frontier bitmap; returns true when this call set it.
  * The plain L2 read first filters the common case of an already-set bit. */
@@ -90,6 +91,25 @@ __device__ __forceinline__ unsigned push4(const Pol &pol, const int4 c)
     return (unsigned)(c.x >= 0) + (c.y >= 0) + (c.z >= 0) + (c.w >= 0);
 }
 
+/* Atomic min (OWNER 0) / max (OWNER 1) and exchange on credits. */
+template <int OWNER>
+__device__ __forceinline__ void atomic_combine(int32_t *a, int32_t v)
+{
+    if (OWNER) atomicMax(a, v);
+    else atomicMin(a, v);
+}
+template <int OWNER>
+__device__ __forceinline__ void atomic_combine(int64_t *a, int64_t v)
+{
+    if (OWNER) atomicMax((long long *)a, (long long)v);
+    else atomicMin((long long *)a, (long long)v);
+}
+__device__ __forceinline__ int32_t atomic_swap(int32_t *a, int32_t v) { return atomicExch(a, v); }
+__device__ __forceinline__ int64_t atomic_swap(int64_t *a, int64_t v)
+{
+    return (int64_t)atomicExch((unsigned long long *)a, (unsigned long long)v);
+}
+
 /* Control block of a persistent solve.  Counters that a round uses are
  * double-buffered by round parity and cleared by the barrier's last
  * arriver, so that no extra pass over them is needed. */
@@ -111,9 +131,10 @@ struct Ctrl {
     /* phase timers (diagnostic mode): warp-nanoseconds summed over warps and
      * rounds in heavy tasks, in word classes, and waiting at the barrier */
     unsigned long long t_heavy, t_light, t_wait;
-    /* direction switching */
-    unsigned long long round_changes[2]; /* raises of round r, by parity         */
-    int next_mode;                       /* 0 sparse, 1 dense, 2 seed then sparse */
+    /* round kinds (lean kernel): raises of round r by parity, the kind the
+     * last arriver picked for the next round, and dense rounds run */
+    unsigned long long round_changes[2];
+    int next_mode;
     int pad2;
     long long dense_rounds;
 };

@@ -273,24 +273,6 @@ __device__ __noinline__ void thread_class(const LiftParams &p, const LiftClass &
     }
 }
 
-template <int OWNER>
-__device__ __forceinline__ void atomic_combine(int32_t *a, int32_t v)
-{
-    if (OWNER) atomicMax(a, v);
-    else atomicMin(a, v);
-}
-template <int OWNER>
-__device__ __forceinline__ void atomic_combine(int64_t *a, int64_t v)
-{
-    if (OWNER) atomicMax((long long *)a, (long long)v);
-    else atomicMin((long long *)a, (long long)v);
-}
-__device__ __forceinline__ int32_t atomic_swap(int32_t *a, int32_t v) { return atomicExch(a, v); }
-__device__ __forceinline__ int64_t atomic_swap(int64_t *a, int64_t v)
-{
-    return (int64_t)atomicExch((unsigned long long *)a, (unsigned long long)v);
-}
-
 /* The last step of a heavy vertex's lift (one warp): compare with the old
  * credit, raise it, clear the vertex's frontier bit, push predecessors. */
 template <class T>
@@ -407,6 +389,30 @@ __device__ __forceinline__ int warp_excl_scan(int v, int lane, int *total)
     return incl - v;
 }
 
+/* The predecessor lists of the raised vertices of one word (lane j owns
+ * vertex u of lane j), dealt to the 32 lanes and pushed four per 128-bit
+ * load. */
+template <class Pol>
+__device__ __forceinline__ void push_raised(const LiftParams &p, const Pol &pol, int u, bool raise, int lane,
+                                            LiftCounters &cnt)
+{
+    int cb = 0, nc = 0;
+    if (raise) {
+        cb = __ldg(p.CP + u) >> 2;
+        nc = (__ldg(p.CP + u + 1) >> 2) - cb;
+    }
+    int ptotal;
+    const int pexcl = warp_excl_scan(nc, lane, &ptotal);
+    cnt.any_new |= ptotal > 0;
+    for (int base = 0; base < ptotal; base += 32) {
+        const int t = base + lane;
+        const int own = owner_of(pexcl, t);
+        const int ocb = __shfl_sync(0xffffffffu, cb, own);
+        const int oex = __shfl_sync(0xffffffffu, pexcl, own);
+        if (t < ptotal) cnt.pushes += push4(pol, __ldg((const int4 *)p.CS + ocb + (t - oex)));
+    }
+}
+
 /* One frontier word of light vertices, warp-cooperative and edge-parallel:
  * lane j owns vertex j of the word; the word's edge pairs are dealt to the
  * 32 lanes, combined per vertex by a segmented shuffle reduction, and the
@@ -458,26 +464,14 @@ __device__ __forceinline__ void light_word(const LiftParams &p, T *F, const Pol 
     }
     cnt.edges += (unsigned long long)real;
     const bool raise = act && old < acc;
-    int cb = 0, nc = 0;
     if (act) {
         cnt.lifts++;
         if (raise) {
             pol.store(F + u, acc);
             cnt.changes++;
-            cb = __ldg(p.CP + u) >> 2;
-            nc = (__ldg(p.CP + u + 1) >> 2) - cb;
         }
     }
-    int ptotal;
-    const int pexcl = warp_excl_scan(nc, lane, &ptotal);
-    cnt.any_new |= ptotal > 0;
-    for (int base = 0; base < ptotal; base += 32) {
-        const int t = base + lane;
-        const int own = owner_of(pexcl, t);
-        const int ocb = __shfl_sync(0xffffffffu, cb, own);
-        const int oex = __shfl_sync(0xffffffffu, pexcl, own);
-        if (t < ptotal) cnt.pushes += push4(pol, __ldg((const int4 *)p.CS + ocb + (t - oex)));
-    }
+    push_raised(p, pol, u, raise, lane, cnt);
 }
 
 /* Two light words at once: the same steps as light_word, with the loads of
@@ -620,6 +614,24 @@ __device__ __noinline__ void light_class(const LiftParams &p, const LiftClass &l
     }
 }
 
+/* The first step of the frontier rounds that follow dense ones: the
+ * predecessors of the vertices raised by the last (recording) dense round,
+ * marked in `ch`, join the frontier `bm`; the marks are consumed. */
+__device__ __noinline__ void seed_words(const LiftParams &p, uint32_t *ch, uint32_t *bm, LiftCounters &cnt)
+{
+    const int lane = threadIdx.x & 31;
+    const int gwarp = (int)((blockIdx.x * (unsigned)blockDim.x + threadIdx.x) >> 5);
+    const int nwarp = (int)((gridDim.x * (unsigned)blockDim.x) >> 5);
+    const int nwords = p.n_pad >> 5;
+    const GridPolicy pol{bm};
+    for (int gw = gwarp; gw < nwords; gw += nwarp) {
+        const uint32_t raised = __ldcg(ch + gw);
+        if (!raised) continue;
+        push_raised(p, pol, (gw << 5) + lane, (raised >> lane) & 1u, lane, cnt);
+        if (lane == 0) __stcg(ch + gw, 0u);
+    }
+}
+
 /* CTA-level processing: the whole CTA lifts one vertex at a time. */
 template <class T, int OWNER>
 __device__ __noinline__ void cta_class(const LiftParams &p, const LiftClass &lc, T *F, uint32_t *cur, uint32_t *nxt,
@@ -713,21 +725,38 @@ __device__ __forceinline__ void run_class(const LiftParams &p, const LiftClass &
     }
 }
 
-/* LEAN: the AUTO layout only (heavy tasks, thread and 8-lane classes),
- * compiled for three CTAs per SM; otherwise every variant, two CTAs per SM. */
+/* LEAN: the AUTO layout only (heavy tasks and light words), compiled for
+ * three CTAs per SM; otherwise every variant, two CTAs per SM.
+ *
+ * Frontier rounds: round r lifts the vertices of B[r&1] and pushes into
+ * B[(r+1)&1].  With round kinds on (LEAN, eg_opts.direction SWITCH) the
+ * kernel hands over to the dense kernel: it starts at round Ctrl::rounds,
+ * runs a seed step first when the dense kernel asked for one, and returns
+ * as soon as the barrier's last arriver picks a dense round (raises of the
+ * round >= dense_min_changes). */
 template <class T, bool LEAN>
 __global__ void __launch_bounds__(LIFT_BLOCK, LEAN ? 3 : 2) k_lift(const __grid_constant__ LiftParams p)
 {
+    __shared__ unsigned long long s_changes;
     Ctrl *c = p.ctrl;
     T *F = (T *)p.F;
     LiftCounters cnt = {0ull, 0ull, 0u, 0u, 0};
-    if (blockIdx.x == 0 && threadIdx.x == 0) c->t_start = globaltimer_ns();
-    for (long long round = 0;; round++) {
+    const bool kinds = LEAN && p.direction == EG_DIRECTION_SWITCH;
+    if (blockIdx.x == 0 && threadIdx.x == 0 && c->t_start == 0ull) c->t_start = globaltimer_ns();
+    if (threadIdx.x == 0) s_changes = 0ull;
+    __syncthreads();
+    const long long round0 = ld_volatile(&c->rounds);
+    for (long long round = round0;; round++) {
         uint32_t *cur = (round & 1) ? p.B1 : p.B0;
         uint32_t *nxt = (round & 1) ? p.B0 : p.B1;
         int *ctr = c->ctr[round & 1];
+        const unsigned changes0 = cnt.changes;
         cnt.any_new = 0;
         unsigned long long t0 = 0, t1 = 0, t2 = 0;
+        if (kinds && round == round0 && ld_volatile(&c->next_mode) == ROUND_SEED) {
+            seed_words(p, (round & 1) ? p.CH0 : p.CH1, cur, cnt);
+            if (!grid_barrier(c, p.wait_limit_ns, [] {})) break;
+        }
         if (p.profile) t0 = globaltimer_ns();
         if (p.num_tasks) heavy_tasks<T>(p, F, cur, nxt, cnt);
         if (p.profile) t1 = globaltimer_ns();
@@ -737,22 +766,36 @@ __global__ void __launch_bounds__(LIFT_BLOCK, LEAN ? 3 : 2) k_lift(const __grid_
             else run_class<T, 0, LEAN>(p, lc, F, cur, nxt, ctr + ci, cnt);
         }
         if (p.profile) t2 = globaltimer_ns();
+        if (kinds) {
+            /* this round's raises: warp sums into shared memory, then one
+             * global add per CTA below */
+            unsigned d = cnt.changes - changes0;
+#pragma unroll
+            for (int off = 16; off > 0; off >>= 1) d += __shfl_xor_sync(0xffffffffu, d, off);
+            if ((threadIdx.x & 31) == 0 && d) atomicAdd(&s_changes, (unsigned long long)d);
+        }
         if (__syncthreads_or(cnt.any_new) && threadIdx.x == 0) c->flag[(round + 1) & 1] = 1;
+        if (kinds && threadIdx.x == 0) {
+            if (s_changes) atomicAdd(&c->round_changes[round & 1], s_changes);
+            s_changes = 0ull;
+        }
         const bool ok = grid_barrier(c, p.wait_limit_ns, [&]() {
             /* last arriver of round `round`: clear this parity's counters
-             * and flag, then decide whether the solve goes on */
+             * and flag, pick the next round's kind, then decide whether the
+             * solve goes on */
             for (int ci = 0; ci < EG_MAX_CLASSES; ci++) c->ctr[round & 1][ci] = 0;
             c->flag[round & 1] = 0;
             c->rounds = round + 1;
-            if (ld_volatile(&c->flag[(round + 1) & 1])) {
-                if (p.max_rounds >= 0 && round + 1 >= p.max_rounds) {
-                    c->stop = (int)EG_ERR_LOOPCAP;
-                } else if (p.timeout_ns && globaltimer_ns() - c->t_start > p.timeout_ns) {
-                    c->stop = (int)EG_ERR_TIMEOUT;
-                } else if (p.cancel && (round & 63) == 0 && ld_volatile(p.cancel)) {
-                    c->stop = (int)EG_ERR_CANCELLED;
-                }
+            const bool more = ld_volatile(&c->flag[(round + 1) & 1]) != 0;
+            if (kinds) {
+                const unsigned long long raised = c->round_changes[round & 1];
+                c->round_changes[(round + 1) & 1] = 0ull;
+                c->next_mode = !more ? ROUND_DONE
+                               : (long long)raised >= p.dense_min_changes ? ROUND_DENSE : ROUND_SPARSE;
+            } else if (!more) {
+                c->next_mode = ROUND_DONE;
             }
+            if (more) check_stop(p, c, round);
         });
         if (p.profile && (threadIdx.x & 31) == 0) {
             const unsigned long long t3 = globaltimer_ns();
@@ -763,6 +806,7 @@ __global__ void __launch_bounds__(LIFT_BLOCK, LEAN ? 3 : 2) k_lift(const __grid_
         if (!ok) break;
         if (ld_volatile(&c->stop)) break;
         if (!ld_volatile(&c->flag[(round + 1) & 1])) break;
+        if (kinds && ld_volatile(&c->next_mode) == ROUND_DENSE) break; /* the dense kernel takes over */
     }
     /* statistics */
     unsigned long long l = cnt.lifts, e = cnt.edges, ch = cnt.changes, pu = cnt.pushes;

@@ -43,15 +43,37 @@ struct LiftParams {
     int *hrem;                 /* per heavy vertex: tasks still to report          */
     int profile;               /* non-zero: accumulate the phase timers of Ctrl    */
     int lean;                  /* AUTO layout: use the lean kernel instantiation   */
-    /* direction switching (lean kernel): a round is dense (every vertex
-     * lifted, no frontier) after >= dense_min_changes raises, and goes back to
-     * the frontier below sparse_max_changes raises */
-    uint32_t *CH0, *CH1;       /* raised-in-round bitmaps, by parity               */
+    /* round kinds (lean layout): frontier rounds in k_lift, rounds over
+     * every vertex in k_lift_dense; the host alternates the two launches */
+    uint32_t *CH0, *CH1;       /* vertices raised in a recording dense round, by parity */
     long long dense_min_changes, sparse_max_changes;
-    int direction;             /* 0 switch, 1 sparse only, 2 dense only           */
-    int light_word_end;        /* words [0, light_word_end) are light             */
-    int words;                 /* frontier words                                  */
+    int direction;             /* eg_direction                                     */
+    /* the dense kernel's pair stream: E4 cut into equal slices of `slice`
+     * pairs (a multiple of 32), one per warp */
+    const uint16_t *PM;        /* per pair: owner << 15 | last pair of its vertex << 14
+                                  | vertex - CB[pair / 32]                        */
+    const int *CB;             /* per 32-pair chunk: the vertex of its first pair  */
+    int npairs;                /* pairs in E4                                      */
+    int slice;                 /* pairs per warp                                   */
+    void *dacc;                /* per vertex cut by slice edges: partial min / max */
+    int *drem;                 /* per cut vertex: slices still to report           */
 };
+
+/* Round kinds, as Ctrl::next_mode holds them between rounds and launches. */
+enum { ROUND_SPARSE = 0, ROUND_DENSE = 1, ROUND_SEED = 2, ROUND_RECORD = 3, ROUND_DONE = 4 };
+
+/* Stop conditions checked by a round's last arriver when work is left: the
+ * round cap, the timeout, and (every 64 rounds) the cancel flag. */
+__device__ __forceinline__ void check_stop(const LiftParams &p, Ctrl *c, long long round)
+{
+    if (p.max_rounds >= 0 && round + 1 >= p.max_rounds) {
+        c->stop = (int)EG_ERR_LOOPCAP;
+    } else if (p.timeout_ns && globaltimer_ns() - c->t_start > p.timeout_ns) {
+        c->stop = (int)EG_ERR_TIMEOUT;
+    } else if (p.cancel && (round & 63) == 0 && ld_volatile(p.cancel)) {
+        c->stop = (int)EG_ERR_CANCELLED;
+    }
+}
 
 /* Edge pairs per heavy task (256 edges). */
 constexpr int kTaskPairs = 128;
@@ -61,6 +83,18 @@ constexpr int kTaskPairs = 128;
 eg_status launch_lift(const LiftParams &p, int credit_bits, cudaStream_t st, int *grid, int *block, int max_ctas);
 /* One-CTA launch for small games (frontier in shared memory). */
 eg_status launch_lift_cta(const LiftParams &p, int credit_bits, cudaStream_t st);
+/* Cooperative launch of the dense-round kernel (eg_dense.cu) with `grid`
+ * CTAs of 512 threads: the grid that p.slice was computed for. */
+eg_status launch_lift_dense(const LiftParams &p, int credit_bits, cudaStream_t st, int grid);
+/* CTAs of a full-occupancy dense launch, at most max_ctas when > 0. */
+eg_status dense_grid(int credit_bits, int max_ctas, int *grid);
+/* Pair-stream metadata PM / CB of a prepared layout; *err (device) is
+ * raised when a chunk's vertex offsets do not fit 14 bits. */
+struct ClassTable;
+void build_pair_meta(const int *P, int n_pad, int npairs, const ClassTable &ct, uint16_t *PM, int *CB, int *err,
+                     cudaStream_t st);
+/* Per-solve reporter counts of the vertices cut by slice edges. */
+void launch_dense_setup(const LiftParams &p, int credit_bits, cudaStream_t st);
 
 }  // namespace eg
 

@@ -70,6 +70,17 @@ typedef enum eg_variant {
     EG_VARIANT_SMEM = 4      /* whole game resident in one CTA's shared memory       */
 } eg_variant;
 
+/* Round kinds of the lean grid kernel (eg_opts.direction).  A sparse round
+ * lifts the frontier and pushes predecessors of raised vertices, as the
+ * reference's worklist does; a dense round lifts every vertex and pushes
+ * nothing.  Both are fair chaotic iterations of the same operator, so the
+ * credits do not depend on the choice. */
+typedef enum eg_direction {
+    EG_DIRECTION_SWITCH = 0, /* dense while many credits rise, sparse otherwise      */
+    EG_DIRECTION_SPARSE = 1,
+    EG_DIRECTION_DENSE = 2
+} eg_direction;
+
 /* A game in compressed sparse row form, vertices 0..num_nodes-1.
  * Owners are given either by a split index (the reference layout:
  * vertices [0, num_nodes0) belong to player 0, the rest to player 1;
@@ -107,6 +118,13 @@ typedef struct eg_opts {
     int32_t profile;             /* non-zero: report the kernel's phase timers        */
     int32_t ctas_per_sm;         /* AUTO layout: 3 = lean kernel at three CTAs per SM,
                                     2 = full kernel at two (0: 3)                     */
+    int32_t direction;           /* lean kernel rounds: 0 switch between frontier
+                                    (sparse) and full (dense) rounds, 1 sparse only,
+                                    2 dense only                                      */
+    int32_t dense_permille;      /* a round after >= this many raises per thousand
+                                    vertices is dense (0: 40)                         */
+    int32_t sparse_permille;     /* a dense round with fewer raises per thousand
+                                    vertices is followed by sparse ones (0: 15)       */
 } eg_opts;
 
 typedef struct eg_stats {
@@ -124,7 +142,8 @@ typedef struct eg_stats {
     int64_t changes;             /* lifts that raised a credit                        */
     int64_t pushes;              /* predecessor entries scanned after those raises    */
     int32_t grid, block;         /* launch shape of the lifting kernel                */
-    int32_t reserved[2];
+    int32_t dense_rounds;        /* rounds that lifted every vertex (no frontier)     */
+    int32_t reserved;
     /* with opts.profile: mean time per warp and round in heavy tasks, in word
      * classes, and waiting at the round barrier (nanoseconds) */
     double  phase_heavy_ns, phase_light_ns, phase_wait_ns;

@@ -93,6 +93,52 @@ def test_cfg2_scaled_variants_and_buckets():
         np.testing.assert_array_equal(f, ref, err_msg=str(v))
 
 
+# Round kinds of the lean grid layout.  With dense_permille=1 and
+# sparse_permille=1000 every frontier round with a few raises hands over to
+# the dense kernel, whose next round records and hands back through a seed
+# step, so every transition runs many times in one solve.
+DIRECTIONS = [
+    dict(direction=eg.DIRECTION_SPARSE),
+    dict(direction=eg.DIRECTION_DENSE),
+    dict(direction=eg.DIRECTION_SWITCH),
+    dict(direction=eg.DIRECTION_SWITCH, dense_permille=1, sparse_permille=1000),
+    dict(direction=eg.DIRECTION_SWITCH, dense_permille=1, sparse_permille=1),
+]
+
+
+@pytest.fixture(scope="module")
+def cfg2_2e14():
+    game = workloads.cfg2(1 << 14)
+    ref, _ = O.eg_solve(game, bits=64)
+    return game, ref
+
+
+@pytest.mark.parametrize("d", DIRECTIONS, ids=vid)
+@pytest.mark.parametrize("bits", [32, 64])
+def test_round_kinds_give_identical_credits(cfg2_2e14, d, bits):
+    game, ref = cfg2_2e14
+    f, st = eg.solve(game, credit_bits=bits, **d)
+    if bits == 32:
+        np.testing.assert_array_equal(f.astype(np.int64), to_top32(ref))
+    else:
+        np.testing.assert_array_equal(f, ref)
+    assert st.grid > 1  # the grid kernel, not the one-CTA one
+    if d["direction"] == eg.DIRECTION_SPARSE:
+        assert st.dense_rounds == 0
+    elif d["direction"] == eg.DIRECTION_DENSE:
+        assert st.dense_rounds == st.rounds
+    elif d.get("sparse_permille") == 1000:
+        # frontier, dense, recording dense, seed + frontier, ...
+        assert st.rounds // 3 <= st.dense_rounds < st.rounds
+
+
+@pytest.mark.parametrize("d", DIRECTIONS[1:4], ids=vid)
+def test_round_kinds_on_heavy_only_clique(d):
+    game = workloads.cfg3()
+    f, st = eg.solve(game, credit_bits=32, **d)
+    assert_exact(game, f, 32)
+
+
 def test_random_small_games_bit_exact():
     kinds = [(1, 3), (2, 60), (4, 16), (5, 40)]
     for seed in range(12):
