@@ -16,8 +16,11 @@ initial frontier, the persistent lifting kernel until the least fixed point.
   e2e    the same metric through the one-call public API eg_solve_i64 with
          pinned host buffers: allocation, host->device copy of the CSR, solve,
          device->host copy of the credits, per step (wall clock)
-  roofline   the lifting kernel's algorithmic bytes / its event time, against
-         the measured HBM copy bandwidth
+  roofline   the dominant kernel (k_lift_dense, the dense rounds): its
+         algorithmic bytes per launch / its mean launch time (CUDA events
+         around each launch, on the solver's stream), against the measured
+         HBM copy bandwidth; `traffic` is the DRAM bytes per launch scaled
+         from an ncu capture of a round-capped solve (profiles/)
   cpu_baseline   the reference's own EG_cpu_solver (oracle/_ref, compiled
          unmodified; serial worklist, 1 core) on a bounded sample of the same
          game: its first P worklist pops (reference --eg P)
@@ -67,6 +70,7 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--variant", type=int, default=0)
+    ap.add_argument("--narrow", action="store_true", help="allow 32-bit device credits where exact")
     ap.add_argument("--max-rounds", type=int, default=-1,
                     help="profiling aid: cap every solve at this many rounds (the line is then not a benchmark)")
     return ap.parse_args()
@@ -145,8 +149,19 @@ def measured_peak():
     return 6650.0, "fallback"
 
 
+def dense_round_bytes(game, credit_bytes: int) -> int:
+    """Algorithmic bytes of one dense round: per edge pair (two out-edges,
+    odd degrees padded) 16 B of {succ, w} x 2 and 2 B of metadata, 4 B per
+    32-pair chunk; per out-edge the successor's credit S; per vertex its own
+    credit S.  (Credit writes, S per raise, are added from the raise count.)"""
+    deg = np.diff(game.row_ptr)
+    npairs = int(((deg + 1) // 2).sum())
+    S = credit_bytes
+    return npairs * 18 + (npairs + 31) // 32 * 4 + game.num_edges * S + game.num_nodes * S
+
+
 def lift_traffic_bytes(st, credit_bytes: int) -> float:
-    """Algorithmic bytes of one lifting-kernel launch:
+    """Algorithmic bytes of the frontier kernel's rounds:
     per scanned edge: successor 4 + weight 4 + successor credit S;
     per lifted vertex: two row offsets 8 + own credit S;
     per raised credit: the write S + two CSC offsets 8;
@@ -380,7 +395,10 @@ def main():
 
     res = eg.ResidentGame(game, device=local)
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.int32, device=f"cuda:{local}")
-    kw = dict(credit_bits=credit_bits, device=local, variant=args.variant, max_rounds=args.max_rounds)
+    # int64 credits on the device, as the workload specifies (--narrow lets
+    # the solver compute in 32 bits where that is exact)
+    kw = dict(credit_bits=credit_bits, device=local, variant=args.variant, max_rounds=args.max_rounds,
+              narrow=args.narrow)
     capped = args.max_rounds >= 0
     for _ in range(args.warmup):
         flush.fill_(1)
@@ -462,20 +480,35 @@ def main():
 
     last = stats[-1]
     peak, peak_kind = measured_peak()
-    lift_bytes = lift_traffic_bytes(last, credit_bits // 8)
-    achieved = lift_bytes / (last.lift_ms / 1e3) / 1e9
+    S = credit_bits // 8
     traffic = None
-    tf = ROOT / "profiles" / "lift_traffic.json"
-    if tf.exists():
-        try:
-            d = json.loads(tf.read_text())
-            if d.get("workload") == cfg["workload"] and d.get("n") == game.num_nodes:
-                traffic = d.get("dram_bytes_per_launch")
-        except (ValueError, KeyError):
-            traffic = None
+    if last.dense_rounds > 0 and last.dense_ms > 0:
+        # the dense-round kernel: mean over its launches in the timed steps
+        d_rounds = sum(s.dense_rounds for s in stats)
+        d_launch = sum(s.dense_launches for s in stats)
+        d_bytes = d_rounds * dense_round_bytes(game, S) + sum(s.dense_changes for s in stats) * S
+        d_ms = sum(s.dense_ms for s in stats)
+        per_launch = d_bytes / d_launch
+        achieved = d_bytes / (d_ms / 1e3) / 1e9
+        kernel = "k_lift_dense (persistent dense-round kernel)"
+        tf = ROOT / "profiles" / "k_lift_dense_traffic.json"
+        if tf.exists():
+            try:
+                d = json.loads(tf.read_text())
+                if d.get("workload") == cfg["workload"] and d.get("n") == game.num_nodes:
+                    traffic = d["dram_bytes_per_round"] * d_rounds / d_launch
+            except (ValueError, KeyError):
+                traffic = None
+        extra = {"launches": d_launch, "rounds_per_launch": d_rounds / d_launch,
+                 "ms_per_launch": d_ms / d_launch, "bytes_per_round": dense_round_bytes(game, S)}
+    else:
+        per_launch = lift_traffic_bytes(last, S)
+        achieved = per_launch / (last.lift_ms / 1e3) / 1e9
+        kernel = "k_lift (persistent frontier kernel)"
+        extra = {}
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                 "traffic": traffic, "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)",
-                "kernel": "k_lift (persistent lifting kernel)", "algorithmic_bytes_per_launch": lift_bytes}
+                "kernel": kernel, "algorithmic_bytes_per_launch": per_launch, **extra}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -489,13 +522,15 @@ def main():
             cfg["profiling_cap_rounds"] = args.max_rounds
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": dev_ms_max / args.steps, "higher_is_better": True,
-                "scaling": "weak", "vs_baseline": None, "dtype": "int64", "data": "synthetic", "config": cfg,
+                "scaling": "weak", "vs_baseline": None, "dtype": f"int{last.credit_bits}", "data": "synthetic",
+                "config": cfg,
                 "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(launches),
                 "clocks": clocks,
                 "solve": {"rounds": last.rounds, "lifts": last.lifts, "edges": last.edges, "changes": last.changes,
                           "pushes": last.pushes, "num_top": last.num_top, "mg": last.mg,
                           "solve_ms": last.solve_ms, "lift_ms": last.lift_ms, "grid": last.grid,
-                          "block": last.block, "wall_s_timed": t_wall}}
+                          "block": last.block, "dense_rounds": last.dense_rounds,
+                          "dense_launches": last.dense_launches, "wall_s_timed": t_wall}}
         print(json.dumps(line), flush=True)
     if dist:
         dist.barrier()

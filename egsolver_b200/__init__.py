@@ -123,9 +123,12 @@ class Stats:
     grid: int
     block: int
     dense_rounds: int
+    dense_launches: int
     phase_heavy_ns: float
     phase_light_ns: float
     phase_wait_ns: float
+    dense_ms: float
+    dense_changes: int
 
     @classmethod
     def from_c(cls, s: _ffi.EgStats) -> "Stats":
@@ -140,7 +143,8 @@ def make_opts(credit_bits: int = 64, variant: int = VARIANT_AUTO, max_rounds: in
               device: int = 0, lanes_per_vertex: int = 0, small_max_deg: int = 0, large_min_deg: int = 0,
               keep_layout: bool = False, cancel: Optional["CancelFlag"] = None, grid_ctas: int = 0,
               task_edges: int = 0, schedule: int = 0, profile: bool = False, ctas_per_sm: int = 0,
-              direction: int = 0, dense_permille: int = 0, sparse_permille: int = 0) -> _ffi.EgOpts:
+              direction: int = 0, dense_permille: int = 0, sparse_permille: int = 0, narrow: bool = False,
+              wide_pairs: bool = False, dense_depth: int = 0) -> _ffi.EgOpts:
     o = _ffi.EgOpts()
     lib().eg_opts_default(C.byref(o))
     o.credit_bits = credit_bits
@@ -160,6 +164,9 @@ def make_opts(credit_bits: int = 64, variant: int = VARIANT_AUTO, max_rounds: in
     o.direction = direction
     o.dense_permille = dense_permille
     o.sparse_permille = sparse_permille
+    o.narrow = 1 if narrow else 0
+    o.wide_pairs = 1 if wide_pairs else 0
+    o.dense_depth = dense_depth
     o.cancel = cancel.ptr if cancel is not None else None
     return o
 

@@ -56,6 +56,9 @@ class EgOpts(C.Structure):
         ("direction", C.c_int32),
         ("dense_permille", C.c_int32),
         ("sparse_permille", C.c_int32),
+        ("narrow", C.c_int32),
+        ("wide_pairs", C.c_int32),
+        ("dense_depth", C.c_int32),
     ]
 
 
@@ -80,10 +83,12 @@ class EgStats(C.Structure):
         ("grid", C.c_int32),
         ("block", C.c_int32),
         ("dense_rounds", C.c_int32),
-        ("reserved", C.c_int32),
+        ("dense_launches", C.c_int32),
         ("phase_heavy_ns", C.c_double),
         ("phase_light_ns", C.c_double),
         ("phase_wait_ns", C.c_double),
+        ("dense_ms", C.c_double),
+        ("dense_changes", C.c_int64),
     ]
 
     def as_dict(self) -> dict:

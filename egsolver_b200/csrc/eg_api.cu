@@ -61,7 +61,7 @@ inline int align32(long long x) { return (int)((x + 31) & ~31LL); }
 struct eg_dgame {
     int device;
     cudaStream_t st;
-    cudaEvent_t ev[4];
+    cudaEvent_t ev[6]; /* solve start, lift start, lift end, solve end; dense launch start / end */
     int n, n0;
     long long m;
     bool has_owner;
@@ -100,6 +100,11 @@ struct eg_dgame {
     void *d_dacc;
     int npairs;
     bool meta_ok;
+    /* the same pairs in 8 bytes when successor and weight fit 32 bits:
+     * (succ << wbits) | (w + wmax) per out-edge */
+    int2 *d_E8;
+    int wbits; /* 0: not packed */
+    long long wmax;
     size_t bytes;
     long long mg;
     int solved_bits;
@@ -194,6 +199,8 @@ static eg_status check_lanes(const eg_opts *o)
         return eg_set_error(EG_ERR_INVALID, "credit_bits must be 32 or 64 (got %d)", o->credit_bits);
     if (o && (o->direction < EG_DIRECTION_SWITCH || o->direction > EG_DIRECTION_DENSE))
         return eg_set_error(EG_ERR_INVALID, "unknown direction %d", o->direction);
+    if (o && (o->dense_depth < 0 || o->dense_depth > 2))
+        return eg_set_error(EG_ERR_INVALID, "dense_depth must be 0, 1 or 2 (got %d)", o->dense_depth);
     if (o && (o->dense_permille < 0 || o->dense_permille > 1000 || o->sparse_permille < 0 || o->sparse_permille > 1000))
         return eg_set_error(EG_ERR_INVALID, "round-kind thresholds must be 0..1000 per mille");
     return EG_OK;
@@ -228,10 +235,10 @@ extern "C" void eg_dgame_free(eg_dgame *g)
     void *ptrs[] = {g->d_rowptr, g->d_succ, g->d_w, g->d_owner, g->d_perm, g->d_iperm, g->d_P, g->d_CP,
                     g->d_CS, g->d_E, g->d_active0, g->d_k0, g->d_v0, g->d_k1, g->d_v1, g->d_scratch,
                     g->d_counts, g->d_mg, g->d_F, g->d_out, g->d_B, g->d_ctrl, g->d_tasks, g->d_hacc,
-                    g->d_hrem, g->d_toff, g->d_PM, g->d_CB, g->d_merr, g->d_drem, g->d_dacc};
+                    g->d_hrem, g->d_toff, g->d_PM, g->d_CB, g->d_merr, g->d_drem, g->d_dacc, g->d_E8};
     for (void *p : ptrs)
         if (p) cudaFree(p);
-    for (int i = 0; i < 4; i++)
+    for (int i = 0; i < 6; i++)
         if (g->ev[i]) cudaEventDestroy(g->ev[i]);
     if (g->st) cudaStreamDestroy(g->st);
     cudaSetDevice(prev);
@@ -265,7 +272,7 @@ static eg_status dgame_alloc(const eg_game *game, const eg_opts *opts, eg_dgame 
     eg_status s = EG_OK;
     cudaError_t e = cudaStreamCreateWithFlags(&g->st, cudaStreamNonBlocking);
     if (e != cudaSuccess) s = eg_set_error(EG_ERR_CUDA, "cudaStreamCreate failed: %s", cudaGetErrorString(e));
-    for (int i = 0; i < 4 && s == EG_OK; i++)
+    for (int i = 0; i < 6 && s == EG_OK; i++)
         if (cudaEventCreate(&g->ev[i]) != cudaSuccess) s = eg_set_error(EG_ERR_CUDA, "cudaEventCreate failed");
     const long long words = g->n_pad_cap / 32 + 2;
     if (s == EG_OK) s = dalloc(g, &g->d_rowptr, (size_t)g->n + 1);
@@ -285,7 +292,7 @@ static eg_status dgame_alloc(const eg_game *game, const eg_opts *opts, eg_dgame 
     if (s == EG_OK) s = dalloc(g, &g->d_v1, (size_t)g->tmp_cap);
     if (s == EG_OK) s = dalloc(g, &g->d_scratch, (size_t)g->scratch_ints);
     if (s == EG_OK) s = dalloc(g, &g->d_counts, (size_t)EG_MAX_CLASSES);
-    if (s == EG_OK) s = dalloc(g, &g->d_mg, 1);
+    if (s == EG_OK) s = dalloc(g, &g->d_mg, 2); /* MG, largest |weight| */
     if (s == EG_OK) s = dalloc(g, (int64_t **)&g->d_F, (size_t)g->n_pad_cap + 64);
     if (s == EG_OK) s = dalloc(g, (int64_t **)&g->d_out, (size_t)g->n);
     if (s == EG_OK) s = dalloc(g, &g->d_B, (size_t)(4 * words)); /* two frontiers, two raised-maps */
@@ -300,6 +307,7 @@ static eg_status dgame_alloc(const eg_game *game, const eg_opts *opts, eg_dgame 
     if (s == EG_OK) s = dalloc(g, &g->d_merr, 1);
     if (s == EG_OK) s = dalloc(g, &g->d_drem, (size_t)g->n_pad_cap);
     if (s == EG_OK) s = dalloc(g, (int64_t **)&g->d_dacc, (size_t)g->n_pad_cap);
+    if (s == EG_OK) s = dalloc(g, &g->d_E8, (size_t)(g->m_pad_cap / 2 + 64));
     if (s != EG_OK) {
         eg_dgame_free(g);
         return s;
@@ -376,20 +384,21 @@ static eg_status dgame_prepare(eg_dgame *g, const eg_opts *opts)
     g->bb = bb;
     memcpy(g->groups, groups, sizeof groups);
     EG_CUDA(cudaMemsetAsync(g->d_counts, 0, sizeof(int) * EG_MAX_CLASSES, st));
-    EG_CUDA(cudaMemsetAsync(g->d_mg, 0, sizeof(unsigned long long), st));
+    EG_CUDA(cudaMemsetAsync(g->d_mg, 0, 2 * sizeof(unsigned long long), st));
     k_classify<<<grid_for(n, kPrepBlock), kPrepBlock, 0, st>>>(n, g->n0, g->d_rowptr, g->d_w, g->d_owner, bb, g->d_k0,
                                                                    g->d_v0, g->d_active0, g->d_mg, g->d_counts);
     g->launches++;
     int counts[EG_MAX_CLASSES];
-    unsigned long long mg = 0;
+    unsigned long long mgw[2] = {0, 0};
     EG_CUDA(cudaMemcpyAsync(counts, g->d_counts, sizeof counts, cudaMemcpyDeviceToHost, st));
-    EG_CUDA(cudaMemcpyAsync(&mg, g->d_mg, sizeof mg, cudaMemcpyDeviceToHost, st));
+    EG_CUDA(cudaMemcpyAsync(mgw, g->d_mg, sizeof mgw, cudaMemcpyDeviceToHost, st));
     int *sk, *sv;
     const int nc = 2 * bb.nb;
     radix_sort_pairs(g->d_k0, g->d_v0, g->d_k1, g->d_v1, n, bits_for(nc - 1), g->d_scratch, st, &sk, &sv);
     g->launches += 3 * ((bits_for(nc - 1) + 7) / 8) + 3;
     EG_CUDA(cudaStreamSynchronize(st));
-    g->mg = (long long)mg;
+    g->mg = (long long)mgw[0];
+    g->wmax = (long long)mgw[1];
     ClassTable ct;
     memset(&ct, 0, sizeof ct);
     ct.nc = nc;
@@ -465,6 +474,16 @@ static eg_status dgame_prepare(eg_dgame *g, const eg_opts *opts)
         EG_CUDA(cudaStreamSynchronize(st));
         g->meta_ok = merr == 0 && g->npairs > 0;
         g->launches += 2;
+        /* 8-byte pairs when ids up to the sentinels and weights in
+         * [-wmax, wmax] share 32 bits */
+        g->wbits = 0;
+        const int sbits = bits_for((long long)n_pad + 1);
+        const int wbits = bits_for(2 * g->wmax);
+        if (g->meta_ok && sbits + wbits <= 32 && !(opts && opts->wide_pairs)) {
+            g->wbits = wbits;
+            launch_pack_pairs((const int4 *)g->d_E, g->npairs, wbits, (int)g->wmax, g->d_E8, st);
+            g->launches++;
+        }
     }
     EG_CUDA(cudaGetLastError());
     g->prepared = true;
@@ -479,12 +498,16 @@ extern "C" eg_status eg_dgame_solve(eg_dgame *g, const eg_opts *opts_in, eg_stat
     const eg_opts *opts = opts_in ? opts_in : &dflt;
     EG_TRY(check_lanes(opts));
     EG_CUDA(cudaSetDevice(g->device));
-    const int bits = opts->credit_bits == 32 ? 32 : 64;
     cudaStream_t st = g->st;
     g->launches = 0;
     g->solved = false;
     EG_CUDA(cudaEventRecord(g->ev[0], st));
     if (!(opts->keep_layout && g->prepared)) EG_TRY(dgame_prepare(g, opts));
+    /* with opts->narrow, a 64-bit request computes in 32 bits when every
+     * finite credit (<= MG) and every difference credit - weight fit: the
+     * same credits, half the bytes, 32-bit warp reductions in dense rounds */
+    const bool fast32 = g->mg + g->wmax < (long long)INT32_MAX;
+    const int bits = opts->credit_bits == 32 ? 32 : (fast32 && opts->narrow) ? 32 : 64;
     if (bits == 32 && g->mg > (long long)INT32_MAX)
         return eg_set_error(EG_ERR_OVERFLOW, "MG = %lld does not fit 32-bit credits", g->mg);
     const int n_pad = g->n_pad;
@@ -561,10 +584,12 @@ extern "C" eg_status eg_dgame_solve(eg_dgame *g, const eg_opts *opts_in, eg_stat
         p.hacc = g->d_hacc;
         p.hrem = g->d_hrem;
     }
-    int grid = 0, block = 0, dgrid = 0;
+    int grid = 0, block = 0, dgrid = 0, dense_launches = 0;
+    double dense_ms = 0.0;
     if (kinds) {
         /* one slice of the pair stream per warp of the dense grid */
-        EG_TRY(dense_grid(bits, opts->grid_ctas, &dgrid));
+        p.dense_depth = opts->dense_depth == 1 ? 1 : 2;
+        EG_TRY(dense_grid(bits, p.dense_depth, opts->grid_ctas, &dgrid));
         const long long warps = (long long)dgrid * 16;
         const long long per = (g->npairs + warps - 1) / warps;
         p.PM = g->d_PM;
@@ -573,6 +598,10 @@ extern "C" eg_status eg_dgame_solve(eg_dgame *g, const eg_opts *opts_in, eg_stat
         p.slice = (int)std::max(32LL, (per + 31) / 32 * 32);
         p.dacc = g->d_dacc;
         p.drem = g->d_drem;
+        p.E8 = g->wbits ? (const int2 *)g->d_E8 : nullptr;
+        p.wbits = g->wbits;
+        p.wbias = (int)g->wmax;
+        p.fast32 = bits == 32 && fast32;
         launch_dense_setup(p, bits, st);
         g->launches++;
     }
@@ -591,9 +620,12 @@ extern "C" eg_status eg_dgame_solve(eg_dgame *g, const eg_opts *opts_in, eg_stat
         int kind = opts->direction == EG_DIRECTION_DENSE ? ROUND_DENSE : ROUND_SPARSE;
         for (;;) {
             if (kind == ROUND_DENSE) {
+                EG_CUDA(cudaEventRecord(g->ev[4], st));
                 EG_TRY(launch_lift_dense(p, bits, st, dgrid));
+                EG_CUDA(cudaEventRecord(g->ev[5], st));
                 grid = dgrid;
                 block = 512;
+                dense_launches++;
             } else {
                 EG_TRY(launch_lift(p, bits, st, &grid, &block, opts->grid_ctas));
             }
@@ -602,6 +634,11 @@ extern "C" eg_status eg_dgame_solve(eg_dgame *g, const eg_opts *opts_in, eg_stat
             EG_CUDA(cudaMemcpyAsync(&tail[0], &g->d_ctrl->stop, sizeof(int), cudaMemcpyDeviceToHost, st));
             EG_CUDA(cudaMemcpyAsync(&tail[1], &g->d_ctrl->next_mode, sizeof(int), cudaMemcpyDeviceToHost, st));
             EG_CUDA(cudaStreamSynchronize(st));
+            if (kind == ROUND_DENSE) {
+                float ms = 0.f;
+                cudaEventElapsedTime(&ms, g->ev[4], g->ev[5]);
+                dense_ms += ms;
+            }
             if (tail[0] || tail[1] == ROUND_DONE) break;
             kind = (tail[1] == ROUND_DENSE || tail[1] == ROUND_RECORD) ? ROUND_DENSE : ROUND_SPARSE;
         }
@@ -622,8 +659,9 @@ extern "C" eg_status eg_dgame_solve(eg_dgame *g, const eg_opts *opts_in, eg_stat
         memset(stats, 0, sizeof *stats);
         stats->mg = g->mg;
         stats->rounds = ctrl.rounds;
-        stats->lifts = (int64_t)ctrl.lifts;
-        stats->edges = (int64_t)ctrl.edges;
+        /* a dense round lifts every vertex and scans every edge once */
+        stats->lifts = (int64_t)ctrl.lifts + (int64_t)ctrl.dense_rounds * g->n;
+        stats->edges = (int64_t)ctrl.edges + (int64_t)ctrl.dense_rounds * g->m;
         stats->num_top = (int64_t)ctrl.num_top;
         stats->solve_ms = solve_ms;
         stats->lift_ms = lift_ms;
@@ -639,7 +677,17 @@ extern "C" eg_status eg_dgame_solve(eg_dgame *g, const eg_opts *opts_in, eg_stat
         stats->grid = grid;
         stats->block = block;
         stats->dense_rounds = (int32_t)ctrl.dense_rounds;
-        if (p.profile) {
+        stats->dense_launches = dense_launches;
+        stats->dense_ms = dense_ms;
+        stats->dense_changes = (int64_t)ctrl.dense_changes;
+        if (p.profile && kinds) {
+            /* dense rounds: mean slice time per warp, mean slowest slice per
+             * round, mean round-to-round time */
+            const double dr = (double)(ctrl.dense_rounds ? ctrl.dense_rounds : 1);
+            stats->phase_light_ns = ctrl.t_light / ((double)dgrid * 16 * dr);
+            stats->phase_heavy_ns = ctrl.t_heavy / dr;
+            stats->phase_wait_ns = ctrl.t_wait / (dr > 1 ? dr - 1 : 1);
+        } else if (p.profile) {
             /* average per warp and round, in nanoseconds */
             const double wr = (double)grid * (block / 32) * (double)(ctrl.rounds ? ctrl.rounds : 1);
             stats->phase_heavy_ns = ctrl.t_heavy / wr;

@@ -149,15 +149,35 @@ void launch_dense_setup(const LiftParams &p, int credit_bits, cudaStream_t st)
 /* The dense-round kernel                                               */
 /* ------------------------------------------------------------------ */
 
-struct DenseCounters {
-    unsigned long long lifts, edges;
-    unsigned changes;
-};
+/* Packs E4's pairs into 8 bytes: per out-edge (succ << wbits) | (w + wbias). */
+__global__ void k_pack_pairs(const int4 *E4, int npairs, int wbits, int wbias, int2 *E8)
+{
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= npairs) return;
+    const int4 q = E4[t];
+    E8[t] = make_int2((int)(((unsigned)q.x << wbits) | (unsigned)(q.y + wbias)),
+                      (int)(((unsigned)q.z << wbits) | (unsigned)(q.w + wbias)));
+}
+
+void launch_pack_pairs(const int4 *E4, int npairs, int wbits, int wbias, int2 *E8, cudaStream_t st)
+{
+    if (npairs <= 0) return;
+    k_pack_pairs<<<(npairs + kMetaBlock - 1) / kMetaBlock, kMetaBlock, 0, st>>>(E4, npairs, wbits, wbias, E8);
+}
+
+/* OMINUS in 32-bit arithmetic, for games where MG + max |w| < 2^31 - 1:
+ * a finite credit minus a weight cannot overflow there, and the wrapped
+ * difference of a = TOP is discarded. */
+__device__ __forceinline__ int32_t ominus_fast(int32_t a, int32_t w, int32_t mg)
+{
+    const int32_t d = (int32_t)((uint32_t)a - (uint32_t)w);
+    return (a < INT32_MAX && d <= mg) ? (d > 0 ? d : 0) : INT32_MAX;
+}
 
 /* A slice's partial value v (actual, not negated) of cut vertex u; the
  * slice that reports last raises the credit.  Returns whether it rose. */
 template <class T>
-__device__ __forceinline__ bool dense_report(const LiftParams &p, T *F, int u, bool own, T v, DenseCounters &cnt)
+__device__ __forceinline__ bool dense_report(const LiftParams &p, T *F, int u, bool own, T v, unsigned &changes)
 {
     T *acc = (T *)p.dacc;
     if (own) atomic_combine<1>(acc + u, v);
@@ -168,11 +188,10 @@ __device__ __forceinline__ bool dense_report(const LiftParams &p, T *F, int u, b
     const T r = atomic_swap(acc + u, own ? (T)0 : credit_traits<T>::top);
     const int b = __ldg(p.P + u) >> 1, e = __ldg(p.P + u + 1) >> 1;
     p.drem[u] = (e - 1) / p.slice - b / p.slice + 1; /* ready for the next round */
-    cnt.lifts++;
     const T old = ld_credit(F + u);
     if (old < r) {
         st_credit(F + u, r);
-        cnt.changes++;
+        changes++;
         return true;
     }
     return false;
@@ -194,107 +213,205 @@ __device__ __forceinline__ void mark_raised(uint32_t *ch, int u, bool raise, int
     }
 }
 
-/* One warp's slice [s0, s1) of the pair stream. */
+/* The two out-edges of pair t: successors and weights. */
+template <bool PACKED>
+__device__ __forceinline__ void load_pair(const LiftParams &p, int t, int4 &q)
+{
+    if (PACKED) {
+        const int2 e = __ldg(p.E8 + t);
+        q = make_int4(e.x, e.y, 0, 0);
+    } else {
+        q = __ldg(p.E4 + t);
+    }
+}
+template <bool PACKED>
+__device__ __forceinline__ void decode_pair(const LiftParams &p, const int4 &q, int &s0, int &w0, int &s1, int &w1)
+{
+    if (PACKED) {
+        const unsigned mask = (1u << p.wbits) - 1u;
+        s0 = (int)((unsigned)q.x >> p.wbits);
+        w0 = (int)((unsigned)q.x & mask) - p.wbias;
+        s1 = (int)((unsigned)q.y >> p.wbits);
+        w1 = (int)((unsigned)q.y & mask) - p.wbias;
+    } else {
+        s0 = q.x;
+        w0 = q.y;
+        s1 = q.z;
+        w1 = q.w;
+    }
+}
+
+/* One 32-pair chunk of a slice as its lanes hold it: the pair, its
+ * metadata and the chunk's first vertex. */
+struct Chunk {
+    int4 q;
+    uint32_t md;
+    int base;
+    bool in;
+};
+
+template <bool PACKED>
+__device__ __forceinline__ void load_chunk(const LiftParams &p, int c0, int s1, int lane, Chunk &k)
+{
+    const int t = c0 + lane;
+    k.in = t < s1;
+    k.q = make_int4(0, 0, 0, 0);
+    k.md = PM_END; /* lanes past the slice end count as ends */
+    k.base = 0;
+    if (k.in) {
+        load_pair<PACKED>(p, t, k.q);
+        k.md = __ldg(p.PM + t);
+    }
+    if (c0 < s1) k.base = __ldg(p.CB + (c0 >> 5));
+}
+
+/* The credits a chunk needs: both successors of the lane's pair and, on the
+ * last pair of a vertex, the vertex's own. */
+template <class T, bool PACKED>
+__device__ __forceinline__ void gather_chunk(const LiftParams &p, const T *F, const Chunk &k, T &fa, T &fb, T &old)
+{
+    fa = fb = old = (T)0;
+    if (k.in) {
+        int sa, wa, sb, wb;
+        decode_pair<PACKED>(p, k.q, sa, wa, sb, wb);
+        fa = ld_credit(F + sa);
+        fb = ld_credit(F + sb);
+        if (k.md & PM_END) old = ld_credit(F + k.base + (int)(k.md & PM_OFF));
+    }
+}
+
+/* Carry of a slice walk: the partial (min-space) value of the vertex that
+ * runs on from the previous chunk. */
 template <class T>
-__device__ __forceinline__ void dense_slice(const LiftParams &p, T *F, uint32_t *ch, bool rec, int s0, int s1,
-                                            int lane, DenseCounters &cnt)
+struct Carry {
+    T val;
+    bool on;   /* the chunk's lane-0 vertex continues from before      */
+    bool cut;  /* that vertex began before this slice: report it       */
+    int u_last;
+    bool own_last;
+};
+
+/* Lifts the vertices of one chunk whose credits have arrived. */
+template <class T, bool FAST, bool PACKED>
+__device__ __forceinline__ void compute_chunk(const LiftParams &p, T *F, uint32_t *ch, bool rec, const Chunk &k, T fa,
+                                              T fb, T old, int lane, uint32_t le_mask, Carry<T> &cr,
+                                              unsigned &changes)
 {
     constexpr T top = credit_traits<T>::top;
+    const int u = k.base + (int)(k.md & PM_OFF);
+    const bool own = (k.md & PM_OWNER) != 0;
+    const bool end = (k.md & PM_END) != 0;
+    T x = top;
+    if (k.in) {
+        int sa, wa, sb, wb;
+        decode_pair<PACKED>(p, k.q, sa, wa, sb, wb);
+        T va, vb;
+        if (FAST) {
+            va = (T)ominus_fast((int32_t)fa, wa, (int32_t)p.mg);
+            vb = (T)ominus_fast((int32_t)fb, wb, (int32_t)p.mg);
+        } else {
+            va = ominus<T>(fa, wa, p.mg);
+            vb = ominus<T>(fb, wb, p.mg);
+        }
+        x = own ? -(va > vb ? va : vb) : (va < vb ? va : vb);
+    }
+    /* inclusive min over each run of one vertex (a max for player 1,
+     * negated), by a shuffle scan */
+    const uint32_t ends = __ballot_sync(0xffffffffu, end);
+    const int head = 31 - __clz(((ends << 1) | 1u) & le_mask);
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const T y = shfl_up_t<T>(x, o);
+        if (lane - o >= head && y < x) x = y;
+    }
+    if (cr.on && head == 0 && cr.val < x) x = cr.val;
+    /* vertices whose last pair is here */
+    bool raise = false;
+    if (k.in && end) {
+        const T v = own ? -x : x;
+        if (head == 0 && cr.cut) {
+            raise = dense_report<T>(p, F, u, own, v, changes);
+        } else if (old < v) {
+            st_credit(F + u, v);
+            changes++;
+            raise = true;
+        }
+    }
+    if (rec) mark_raised(ch, u, raise, lane);
+    /* the last lane's vertex runs on into the next chunk? */
+    const bool open = !(ends >> 31);
+    cr.cut = open && cr.cut && (ends & 0x7fffffffu) == 0u;
+    cr.on = open;
+    cr.val = shfl_t<T>(x, 31);
+    cr.u_last = u;
+    cr.own_last = own;
+}
+
+/* One warp's slice [s0, s1) of the pair stream.  FAST (32-bit credits
+ * whose differences fit 32 bits): 32-bit OMINUS.  PACKED: 8-byte pairs.
+ * DEPTH 1: the next chunk's pairs load while a chunk's credits are
+ * gathered and reduced; DEPTH 2: also the next chunk's credits are in
+ * flight while a chunk is reduced (more registers: two CTAs per SM). */
+template <class T, bool FAST, bool PACKED, int DEPTH>
+__device__ __forceinline__ void dense_slice(const LiftParams &p, T *F, uint32_t *ch, bool rec, int s0, int s1,
+                                            int lane, unsigned &changes)
+{
     if (s0 >= s1) return;
     const uint32_t le_mask = 0xffffffffu >> (31 - lane);
+    Carry<T> cr;
     /* the vertex of the slice's first pair began in an earlier slice? */
-    bool carry_on = s0 > 0 && !(__ldg(p.PM + s0 - 1) & PM_END);
-    bool carry_cut = carry_on;
-    T carry = top; /* min-space partial of the carried vertex */
-    int carry_u = 0;
-    bool carry_own = false;
-    /* chunk 0, then each iteration loads the next chunk before it works */
-    int t = s0 + lane;
-    bool in = t < s1;
-    int4 q = make_int4(0, 0, 0, 0);
-    uint32_t md = PM_END;
-    if (in) {
-        q = __ldg(p.E4 + t);
-        md = __ldg(p.PM + t);
-    }
-    int base = __ldg(p.CB + (s0 >> 5));
-    for (int c0 = s0; c0 < s1; c0 += 32) {
-        const int tn = c0 + 32 + lane;
-        const bool inn = tn < s1;
-        int4 qn = make_int4(0, 0, 0, 0);
-        uint32_t mdn = PM_END;
-        int basen = 0;
-        if (inn) {
-            qn = __ldg(p.E4 + tn);
-            mdn = __ldg(p.PM + tn);
+    cr.on = s0 > 0 && !(__ldg(p.PM + s0 - 1) & PM_END);
+    cr.cut = cr.on;
+    cr.val = credit_traits<T>::top;
+    cr.u_last = 0;
+    cr.own_last = false;
+    Chunk k0, k1;
+    load_chunk<PACKED>(p, s0, s1, lane, k0);
+    if (DEPTH == 1) {
+        for (int c0 = s0; c0 < s1; c0 += 32) {
+            load_chunk<PACKED>(p, c0 + 32, s1, lane, k1);
+            T fa, fb, old;
+            gather_chunk<T, PACKED>(p, F, k0, fa, fb, old);
+            compute_chunk<T, FAST, PACKED>(p, F, ch, rec, k0, fa, fb, old, lane, le_mask, cr, changes);
+            k0 = k1;
         }
-        if (c0 + 32 < s1) basen = __ldg(p.CB + ((c0 + 32) >> 5));
-
-        const int u = base + (int)(md & PM_OFF);
-        const bool own = (md & PM_OWNER) != 0;
-        const bool end = (md & PM_END) != 0; /* lanes past the slice end count as ends */
-        T x = top, old = (T)0;
-        if (in) {
-            const T f0 = ld_credit(F + q.x), f1 = ld_credit(F + q.z);
-            if (end) old = ld_credit(F + u);
-            const T v0 = ominus<T>(f0, q.y, p.mg), v1 = ominus<T>(f1, q.w, p.mg);
-            x = own ? -(v0 > v1 ? v0 : v1) : (v0 < v1 ? v0 : v1);
-            cnt.edges += 1ull + (q.z < p.n_pad);
+    } else {
+        load_chunk<PACKED>(p, s0 + 32, s1, lane, k1);
+        T fa0, fb0, old0;
+        gather_chunk<T, PACKED>(p, F, k0, fa0, fb0, old0);
+        for (int c0 = s0; c0 < s1; c0 += 32) {
+            Chunk k2;
+            load_chunk<PACKED>(p, c0 + 64, s1, lane, k2);
+            T fa1, fb1, old1;
+            gather_chunk<T, PACKED>(p, F, k1, fa1, fb1, old1);
+            compute_chunk<T, FAST, PACKED>(p, F, ch, rec, k0, fa0, fb0, old0, lane, le_mask, cr, changes);
+            k0 = k1;
+            k1 = k2;
+            fa0 = fa1;
+            fb0 = fb1;
+            old0 = old1;
         }
-        /* segmented inclusive min over runs of one vertex */
-        const uint32_t ends = __ballot_sync(0xffffffffu, end);
-        const int head = 31 - __clz(((ends << 1) | 1u) & le_mask);
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            const T y = shfl_up_t<T>(x, o);
-            if (lane - o >= head && y < x) x = y;
-        }
-        if (carry_on && head == 0 && carry < x) x = carry;
-        /* vertices whose last pair is here */
-        bool raise = false;
-        if (in && end) {
-            const T v = own ? -x : x;
-            if (head == 0 && carry_cut) {
-                raise = dense_report<T>(p, F, u, own, v, cnt);
-            } else {
-                cnt.lifts++;
-                if (old < v) {
-                    st_credit(F + u, v);
-                    cnt.changes++;
-                    raise = true;
-                }
-            }
-        }
-        if (rec) mark_raised(ch, u, raise, lane);
-        /* the last lane's vertex runs on into the next chunk? */
-        const bool open = !(ends >> 31);
-        carry_cut = open && carry_cut && (ends & 0x7fffffffu) == 0u;
-        carry_on = open;
-        carry = shfl_t<T>(x, 31);
-        carry_u = __shfl_sync(0xffffffffu, u, 31);
-        carry_own = __shfl_sync(0xffffffffu, (int)own, 31) != 0;
-        q = qn;
-        md = mdn;
-        base = basen;
-        in = inn;
     }
     /* the last vertex goes on in the next slice: report its part */
-    if (carry_on && lane == 0) {
-        const bool r = dense_report<T>(p, F, carry_u, carry_own, carry_own ? -carry : carry, cnt);
-        if (rec && r) atomicOr(ch + (carry_u >> 5), 1u << (carry_u & 31));
+    const int cu = __shfl_sync(0xffffffffu, cr.u_last, 31);
+    const bool cown = __shfl_sync(0xffffffffu, (int)cr.own_last, 31) != 0;
+    if (cr.on && lane == 0) {
+        const bool r = dense_report<T>(p, F, cu, cown, cown ? -cr.val : cr.val, changes);
+        if (rec && r) atomicOr(ch + (cu >> 5), 1u << (cu & 31));
     }
 }
 
 /* Persistent dense rounds from round Ctrl::rounds until the last arriver
  * picks another kind: ROUND_DONE (no raise: solved), or ROUND_SEED after a
- * recording round below sparse_max_changes. */
-template <class T>
-__global__ void __launch_bounds__(DENSE_BLOCK, 3) k_lift_dense(const __grid_constant__ LiftParams p)
+ * recording round below sparse_max_changes.  Lifts and scanned edges are
+ * not counted here: a dense round lifts every vertex and scans every edge. */
+template <class T, bool FAST, bool PACKED, int DEPTH>
+__global__ void __launch_bounds__(DENSE_BLOCK, DEPTH == 1 ? 3 : 2) k_lift_dense(const __grid_constant__ LiftParams p)
 {
-    __shared__ unsigned long long s_changes;
+    __shared__ unsigned long long s_changes, s_busy, s_busy_max;
     Ctrl *c = p.ctrl;
     T *F = (T *)p.F;
-    DenseCounters cnt = {0ull, 0ull, 0u};
+    unsigned changes = 0u;
     const int lane = threadIdx.x & 31;
     const int gthr = (int)(blockIdx.x * blockDim.x + threadIdx.x);
     const int nthr = (int)(gridDim.x * blockDim.x);
@@ -303,7 +420,7 @@ __global__ void __launch_bounds__(DENSE_BLOCK, 3) k_lift_dense(const __grid_cons
     const int s1 = (int)(sl + p.slice < p.npairs ? sl + p.slice : p.npairs);
     const int words = p.n_pad >> 5;
     if (blockIdx.x == 0 && threadIdx.x == 0 && c->t_start == 0ull) c->t_start = globaltimer_ns();
-    if (threadIdx.x == 0) s_changes = 0ull;
+    if (threadIdx.x == 0) s_changes = s_busy = s_busy_max = 0ull;
     __syncthreads();
     const long long round0 = ld_volatile(&c->rounds);
     for (long long round = round0;; round++) {
@@ -317,9 +434,15 @@ __global__ void __launch_bounds__(DENSE_BLOCK, 3) k_lift_dense(const __grid_cons
             if (round == round0) __stcg(cur + w, 0u);
             __stcg(chn + w, 0u);
         }
-        const unsigned changes0 = cnt.changes;
-        dense_slice<T>(p, F, ch, kind == ROUND_RECORD, s0, s1, lane, cnt);
-        unsigned d = cnt.changes - changes0;
+        const unsigned changes0 = changes;
+        const unsigned long long t0 = p.profile ? globaltimer_ns() : 0ull;
+        dense_slice<T, FAST, PACKED, DEPTH>(p, F, ch, kind == ROUND_RECORD, s0, s1, lane, changes);
+        if (p.profile && lane == 0) {
+            const unsigned long long dt = globaltimer_ns() - t0;
+            atomicAdd(&s_busy, dt);
+            atomicMax(&s_busy_max, dt);
+        }
+        unsigned d = changes - changes0;
 #pragma unroll
         for (int off = 16; off > 0; off >>= 1) d += __shfl_xor_sync(0xffffffffu, d, off);
         if (lane == 0 && d) atomicAdd(&s_changes, (unsigned long long)d);
@@ -327,13 +450,27 @@ __global__ void __launch_bounds__(DENSE_BLOCK, 3) k_lift_dense(const __grid_cons
         if (threadIdx.x == 0) {
             if (s_changes) atomicAdd(&c->round_changes[round & 1], s_changes);
             s_changes = 0ull;
+            if (p.profile) {
+                atomicAdd(&c->t_light, s_busy);
+                atomicMax(&c->round_max[round & 1], s_busy_max);
+                s_busy = s_busy_max = 0ull;
+            }
         }
         const bool ok = grid_barrier(c, p.wait_limit_ns, [&]() {
             c->flag[round & 1] = 0;
             c->rounds = round + 1;
             c->dense_rounds++;
+            if (p.profile) {
+                c->t_heavy += c->round_max[round & 1]; /* the slowest slice of the round */
+                c->round_max[round & 1] = 0ull;
+                const unsigned long long now = globaltimer_ns();
+                if (c->t_round_prev) c->t_wait += now - c->t_round_prev; /* round to round */
+                c->t_round_prev = now;
+            }
             const unsigned long long raised = c->round_changes[round & 1];
             c->round_changes[(round + 1) & 1] = 0ull;
+            c->changes += raised;
+            c->dense_changes += raised;
             int next;
             if (raised == 0ull) {
                 next = ROUND_DONE;
@@ -353,31 +490,37 @@ __global__ void __launch_bounds__(DENSE_BLOCK, 3) k_lift_dense(const __grid_cons
         const int nk = ld_volatile(&c->next_mode);
         if (nk != ROUND_DENSE && nk != ROUND_RECORD) break;
     }
-    unsigned long long l = cnt.lifts, e = cnt.edges, chg = cnt.changes;
-#pragma unroll
-    for (int off = 16; off > 0; off >>= 1) {
-        l += __shfl_xor_sync(0xffffffffu, l, off);
-        e += __shfl_xor_sync(0xffffffffu, e, off);
-        chg += __shfl_xor_sync(0xffffffffu, chg, off);
-    }
-    if (lane == 0) {
-        atomicAdd(&c->lifts, l);
-        atomicAdd(&c->edges, e);
-        atomicAdd(&c->changes, chg);
-    }
 }
 
-static const void *dense_fn(int credit_bits)
+template <class T, bool FAST, bool PACKED>
+static const void *dense_fn_depth(int depth)
 {
-    return credit_bits == 32 ? (const void *)k_lift_dense<int32_t> : (const void *)k_lift_dense<int64_t>;
+    return depth == 2 ? (const void *)k_lift_dense<T, FAST, PACKED, 2> : (const void *)k_lift_dense<T, FAST, PACKED, 1>;
 }
 
-eg_status dense_grid(int credit_bits, int max_ctas, int *grid)
+template <class T, bool FAST>
+static const void *dense_fn_packed(bool packed, int depth)
+{
+    return packed ? dense_fn_depth<T, FAST, true>(depth) : dense_fn_depth<T, FAST, false>(depth);
+}
+
+static const void *dense_fn(const LiftParams &p, int credit_bits)
+{
+    const bool packed = p.E8 != nullptr;
+    if (credit_bits == 64) return dense_fn_packed<int64_t, false>(packed, p.dense_depth);
+    return p.fast32 ? dense_fn_packed<int32_t, true>(packed, p.dense_depth)
+                    : dense_fn_packed<int32_t, false>(packed, p.dense_depth);
+}
+
+eg_status dense_grid(int credit_bits, int depth, int max_ctas, int *grid)
 {
     int dev = 0, sms = 0, per_sm = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    cudaError_t err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, dense_fn(credit_bits), DENSE_BLOCK, 0);
+    /* the instantiations of one depth share their launch bounds */
+    const void *fn = credit_bits == 32 ? dense_fn_depth<int32_t, true, true>(depth)
+                                       : dense_fn_depth<int64_t, false, false>(depth);
+    cudaError_t err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, DENSE_BLOCK, 0);
     if (err != cudaSuccess || per_sm < 1)
         return eg_set_error(EG_ERR_CUDA, "occupancy query for the dense kernel failed: %s", cudaGetErrorString(err));
     int g = sms * per_sm;
@@ -388,8 +531,15 @@ eg_status dense_grid(int credit_bits, int max_ctas, int *grid)
 
 eg_status launch_lift_dense(const LiftParams &p, int credit_bits, cudaStream_t st, int grid)
 {
+    const void *fn = dense_fn(p, credit_bits);
+    int per_sm = 0, dev = 0, sms = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaError_t err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, DENSE_BLOCK, 0);
+    if (err != cudaSuccess || per_sm * sms < grid)
+        return eg_set_error(EG_ERR_CUDA, "the dense kernel cannot hold %d co-resident CTAs", grid);
     void *args[] = {(void *)&p};
-    cudaError_t err = cudaLaunchCooperativeKernel(dense_fn(credit_bits), dim3(grid), dim3(DENSE_BLOCK), args, 0, st);
+    err = cudaLaunchCooperativeKernel(fn, dim3(grid), dim3(DENSE_BLOCK), args, 0, st);
     if (err != cudaSuccess)
         return eg_set_error(EG_ERR_CUDA, "cooperative launch of the dense kernel failed: %s", cudaGetErrorString(err));
     return EG_OK;

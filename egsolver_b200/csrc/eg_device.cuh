@@ -137,6 +137,9 @@ struct Ctrl {
     int next_mode;
     int pad2;
     long long dense_rounds;
+    unsigned long long dense_changes;
+    unsigned long long round_max[2];   /* diagnostic: slowest slice of a dense round */
+    unsigned long long t_round_prev;   /* diagnostic: globaltimer at the last round end */
 };
 
 /* Grid barrier for a cooperative launch.  Every wait is bounded by

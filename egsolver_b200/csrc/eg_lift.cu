@@ -797,7 +797,7 @@ __global__ void __launch_bounds__(LIFT_BLOCK, LEAN ? 3 : 2) k_lift(const __grid_
             }
             if (more) check_stop(p, c, round);
         });
-        if (p.profile && (threadIdx.x & 31) == 0) {
+        if (p.profile && !kinds && (threadIdx.x & 31) == 0) {
             const unsigned long long t3 = globaltimer_ns();
             atomicAdd(&c->t_heavy, t1 - t0);
             atomicAdd(&c->t_light, t2 - t1);

@@ -57,6 +57,10 @@ struct LiftParams {
     int slice;                 /* pairs per warp                                   */
     void *dacc;                /* per vertex cut by slice edges: partial min / max */
     int *drem;                 /* per cut vertex: slices still to report           */
+    const int2 *E8;            /* the pairs packed in 8 bytes, or null             */
+    int wbits, wbias;          /* packed edge: (succ << wbits) | (w + wbias)       */
+    int fast32;                /* 32-bit credits whose differences fit 32 bits     */
+    int dense_depth;           /* chunks in flight per warp: 1 (3 CTAs per SM) or 2 */
 };
 
 /* Round kinds, as Ctrl::next_mode holds them between rounds and launches. */
@@ -86,13 +90,16 @@ eg_status launch_lift_cta(const LiftParams &p, int credit_bits, cudaStream_t st)
 /* Cooperative launch of the dense-round kernel (eg_dense.cu) with `grid`
  * CTAs of 512 threads: the grid that p.slice was computed for. */
 eg_status launch_lift_dense(const LiftParams &p, int credit_bits, cudaStream_t st, int grid);
-/* CTAs of a full-occupancy dense launch, at most max_ctas when > 0. */
-eg_status dense_grid(int credit_bits, int max_ctas, int *grid);
+/* CTAs of a full-occupancy dense launch of pipeline depth 1 or 2, at most
+ * max_ctas when > 0. */
+eg_status dense_grid(int credit_bits, int depth, int max_ctas, int *grid);
 /* Pair-stream metadata PM / CB of a prepared layout; *err (device) is
  * raised when a chunk's vertex offsets do not fit 14 bits. */
 struct ClassTable;
 void build_pair_meta(const int *P, int n_pad, int npairs, const ClassTable &ct, uint16_t *PM, int *CB, int *err,
                      cudaStream_t st);
+/* Packs the 16-byte pairs of E4 into 8 bytes (E8). */
+void launch_pack_pairs(const int4 *E4, int npairs, int wbits, int wbias, int2 *E8, cudaStream_t st);
 /* Per-solve reporter counts of the vertices cut by slice edges. */
 void launch_dense_setup(const LiftParams &p, int credit_bits, cudaStream_t st);
 

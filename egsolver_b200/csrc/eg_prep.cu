@@ -240,19 +240,21 @@ __global__ void k_classify(int n, int n0, const long long *row_ptr, const int *w
                            unsigned long long *mg_acc, int *class_count)
 {
     __shared__ int s_cnt[EG_MAX_CLASSES];
-    __shared__ unsigned long long s_mg;
+    __shared__ unsigned long long s_mg, s_wmax;
     if (threadIdx.x < EG_MAX_CLASSES) s_cnt[threadIdx.x] = 0;
-    if (threadIdx.x == 0) s_mg = 0;
+    if (threadIdx.x == 0) s_mg = s_wmax = 0;
     __syncthreads();
-    unsigned long long mg_local = 0;
+    unsigned long long mg_local = 0, wmax_local = 0;
     for (long long v = (long long)blockIdx.x * blockDim.x + threadIdx.x; v < n; v += (long long)gridDim.x * blockDim.x) {
         const long long b = row_ptr[v], e = row_ptr[v + 1];
         const long long deg = e - b;
         const int own = owner ? (int)owner[v] : (v >= n0 ? 1 : 0);
-        int worst = 0; /* max(0, -min weight) */
+        long long worst = 0; /* max(0, -min weight) */
         bool any_neg = false, all_neg = true;
         for (long long j = b; j < e; j++) {
-            const int x = w[j];
+            const long long x = w[j];
+            const unsigned long long ax = (unsigned long long)(x < 0 ? -x : x);
+            if (ax > wmax_local) wmax_local = ax;
             if (x < 0) {
                 any_neg = true;
                 if (-x > worst) worst = -x;
@@ -271,9 +273,13 @@ __global__ void k_classify(int n, int n0, const long long *row_ptr, const int *w
         atomicAdd(&s_cnt[c], 1);
     }
     atomicAdd(&s_mg, mg_local);
+    atomicMax(&s_wmax, wmax_local);
     __syncthreads();
     if (threadIdx.x < EG_MAX_CLASSES && s_cnt[threadIdx.x]) atomicAdd(&class_count[threadIdx.x], s_cnt[threadIdx.x]);
-    if (threadIdx.x == 0) atomicAdd(mg_acc, s_mg);
+    if (threadIdx.x == 0) {
+        atomicAdd(mg_acc, s_mg);
+        atomicMax(mg_acc + 1, s_wmax); /* largest |weight| */
+    }
 }
 
 /* sorted position i (class-major, original order inside a class) -> new id */

@@ -125,6 +125,13 @@ typedef struct eg_opts {
                                     vertices is dense (0: 40)                         */
     int32_t sparse_permille;     /* a dense round with fewer raises per thousand
                                     vertices is followed by sparse ones (0: 15)       */
+    int32_t narrow;              /* non-zero: a 64-bit solve computes in 32 bits when
+                                    MG + max |weight| < 2^31 - 1 (identical credits;
+                                    eg_dgame_credits_device then reports 32)          */
+    int32_t wide_pairs;          /* non-zero: dense rounds read 16-byte edge pairs
+                                    even when successor and weight fit 32 bits        */
+    int32_t dense_depth;         /* chunks in flight per warp in dense rounds: 1 (three
+                                    CTAs per SM) or 2 (two CTAs per SM); 0: 2         */
 } eg_opts;
 
 typedef struct eg_stats {
@@ -136,17 +143,21 @@ typedef struct eg_stats {
     double  solve_ms;            /* device time of the solve (transpose included)    */
     double  lift_ms;             /* device time of the lifting loop alone            */
     int64_t kernel_launches;     /* kernels launched by the solve                     */
-    int32_t credit_bits;         /* width actually used                               */
+    int32_t credit_bits;         /* width of the credits on the device                 */
     int32_t variant_small, variant_mid, variant_large; /* variants used per bucket   */
     int32_t small_max_deg, large_min_deg;               /* bucket bounds used         */
     int64_t changes;             /* lifts that raised a credit                        */
     int64_t pushes;              /* predecessor entries scanned after those raises    */
     int32_t grid, block;         /* launch shape of the lifting kernel                */
     int32_t dense_rounds;        /* rounds that lifted every vertex (no frontier)     */
-    int32_t reserved;
-    /* with opts.profile: mean time per warp and round in heavy tasks, in word
-     * classes, and waiting at the round barrier (nanoseconds) */
+    int32_t dense_launches;      /* launches of the dense-round kernel                */
+    /* with opts.profile, in nanoseconds.  Frontier rounds only: mean time per
+     * warp and round in heavy tasks, in word classes, and waiting at the round
+     * barrier.  With dense rounds: the slowest slice per dense round (heavy),
+     * the mean slice per warp (light), and the mean round-to-round time (wait) */
     double  phase_heavy_ns, phase_light_ns, phase_wait_ns;
+    double  dense_ms;            /* device time of the dense-round kernel's launches  */
+    int64_t dense_changes;       /* credits raised in dense rounds                    */
 } eg_stats;
 
 /* ------------------------------------------------------------------ */

@@ -132,6 +132,51 @@ def test_round_kinds_give_identical_credits(cfg2_2e14, d, bits):
         assert st.rounds // 3 <= st.dense_rounds < st.rounds
 
 
+# Data paths of the dense rounds: 64-bit credits with a shuffle scan, or
+# (narrow, when MG + max|w| fits) 32-bit credits with warp reductions; 8-byte
+# or 16-byte edge pairs.
+DENSE_PATHS = [dict(), dict(wide_pairs=True), dict(narrow=True), dict(narrow=True, wide_pairs=True),
+               dict(dense_depth=1), dict(dense_depth=1, narrow=True, wide_pairs=True)]
+
+
+@pytest.mark.parametrize("d", DENSE_PATHS, ids=lambda d: vid(d) or "default")
+@pytest.mark.parametrize("direction", [eg.DIRECTION_SWITCH, eg.DIRECTION_DENSE])
+def test_dense_data_paths_give_identical_credits(cfg2_2e14, d, direction):
+    game, ref = cfg2_2e14
+    f, st = eg.solve(game, credit_bits=64, direction=direction, **d)
+    np.testing.assert_array_equal(f, ref)
+    assert st.credit_bits == (32 if d.get("narrow") else 64)
+    assert st.dense_rounds > 0 and st.dense_launches >= 1
+
+
+def big_weight_game():
+    """cfg2 at n = 2^14 with weights scaled so that MG fits 31 bits but
+    MG + max|w| does not: 32-bit credits must take the 64-bit difference."""
+    g = workloads.cfg2(1 << 14)
+    w = g.weight.astype(np.int64) * 302
+    deg = np.diff(g.row_ptr)
+    src = np.repeat(np.arange(g.num_nodes), deg)
+    worst = np.zeros(g.num_nodes, np.int64)
+    np.maximum.at(worst, src, np.maximum(0, -w))
+    v = int(np.argmax(worst))
+    j = g.row_ptr[v] + int(np.argmin(w[g.row_ptr[v]:g.row_ptr[v + 1]]))
+    w[j] = -(worst[v] + (2**31 - 1) - 150000 - worst.sum())
+    return eg.Game(row_ptr=g.row_ptr, succ=g.succ, weight=w.astype(np.int32), num_nodes0=g.num_nodes0)
+
+
+def test_dense_rounds_with_mg_near_the_32_bit_limit():
+    game = big_weight_game()
+    mg = eg.compute_mg(game, 64)
+    assert mg <= 2**31 - 1 < mg + int(np.abs(game.weight).max())
+    ref, _ = O.eg_solve(game, bits=64)
+    f32, st32 = eg.solve(game, credit_bits=32)
+    assert st32.credit_bits == 32 and st32.dense_rounds > 0
+    np.testing.assert_array_equal(f32.astype(np.int64), to_top32(ref))
+    f64, st64 = eg.solve(game, credit_bits=64, narrow=True)
+    assert st64.credit_bits == 64  # no narrowing: MG + max|w| does not fit
+    np.testing.assert_array_equal(f64, ref)
+
+
 @pytest.mark.parametrize("d", DIRECTIONS[1:4], ids=vid)
 def test_round_kinds_on_heavy_only_clique(d):
     game = workloads.cfg3()
