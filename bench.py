@@ -59,11 +59,14 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", choices=["cfg1", "cfg2", "cfg3", "cfg4", "cfg5"], default="cfg2")
-    ap.add_argument("--games", type=int, default=4096, help="cfg4: number of games")
-    ap.add_argument("--plain-sample", type=int, default=24, help="cfg4/cfg5: requests timed on the plain path")
-    ap.add_argument("--requests", type=int, default=200, help="cfg5: requests per arrival rate")
-    ap.add_argument("--rates", type=str, default="2,8,32,128", help="cfg5: arrival rates (requests/s) swept")
-    ap.add_argument("--n-max", type=int, default=1 << 19, help="cfg5: largest request game")
+    ap.add_argument("--games", type=int, default=64,
+                    help="cfg4: the first G games of the 4096-game stream (same seeds)")
+    ap.add_argument("--plain-sample", type=int, default=24, help="cfg4: (game, threshold) pairs timed on the plain path")
+    ap.add_argument("--plain-budget-s", type=float, default=45.0,
+                    help="cfg4/cfg5: wall-clock budget of the plain-path measurements")
+    ap.add_argument("--requests", type=int, default=16, help="cfg5: requests per arrival rate (at most)")
+    ap.add_argument("--rates", type=str, default="4,32", help="cfg5: arrival rates (requests/s) swept")
+    ap.add_argument("--n-max", type=int, default=1 << 13, help="cfg5: largest request game")
     ap.add_argument("--n", type=int, default=0, help="override the vertex count (smaller cases)")
     ap.add_argument("--e2e-steps", type=int, default=0, help="e2e steps (default: --steps)")
     ap.add_argument("--cpu-sample-s", type=float, default=10.0)
@@ -238,6 +241,11 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+def progress(msg: str) -> None:
+    """A progress line on stderr (the JSON result line stays alone on stdout)."""
+    print(f"[bench] {msg}", file=sys.stderr, flush=True)
+
+
 def run_batched(args):
     """cfg4: many uneven games x K=8 mean-payoff thresholds in one persistent
     launch (CUDA-graph replay, autotuned CTA size) against the plain path that
@@ -255,15 +263,19 @@ def run_batched(args):
     b = eg.Batch(games, thresholds=K, scale=d, use_graph=True)
     b.set_thresholds(p)
     setup_s = time.perf_counter() - t0
+    progress(f"batch of {G} games uploaded in {setup_s:.1f} s")
     block = b.tune()
+    progress(f"tuned: block {block}")
     for _ in range(args.warmup):
-        b.solve()
+        _, wst = b.solve()
+        progress(f"warm-up solve {wst.solve_ms:.1f} ms")
     sampler = ClockSampler(0)
     times, stats = [], []
     for _ in range(args.steps):
         _, st = b.solve()
         times.append(st.solve_ms)
         stats.append(st)
+        progress(f"timed solve {st.solve_ms:.1f} ms")
     clocks = sampler.stop()
     ms = sum(times) / len(times)
     value = G / (ms / 1e3)
@@ -280,17 +292,22 @@ def run_batched(args):
     # plain path: one single-game solve per (game, threshold) on a seeded sample
     pick = rng.choice(G, size=min(args.plain_sample, G), replace=False)
     plain_ms, plain_pairs = 0.0, 0
+    t_plain = time.perf_counter()
     for g in pick:
+        if plain_pairs and time.perf_counter() - t_plain > args.plain_budget_s:
+            break
         k = int(rng.integers(0, K))
         tg = eg.threshold_game(games[g], int(p[g, k]), d)
         with eg.ResidentGame(tg) as r:
             _, pst = r.solve()
             plain_ms += pst.solve_ms
             plain_pairs += 1
+            progress(f"plain pair {plain_pairs}: game {g} n={tg.num_nodes} {pst.solve_ms:.1f} ms")
     plain = plain_pairs / K / (plain_ms / 1e3)
     last = stats[-1]
     b.free()
-    line = {"metric": "batched games/s (cfg4: 4096 uneven games x 8 mean-payoff thresholds, one launch)",
+    line = {"metric": f"batched games/s (cfg4 stream, first {G} of 4096 uneven games x 8 mean-payoff thresholds, "
+                      "one launch)",
             "value": value, "unit": "games/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int64",
             "data": "synthetic",
@@ -315,9 +332,14 @@ def run_served(args):
 
     reqs = workloads.cfg5_requests(args.requests, n_max=args.n_max)
     rng = np.random.default_rng(11)
-    # plain service time of every request: K single-game solves
+    # plain service time of every request: K single-game solves; the stream
+    # is cut after the request that exhausts the plain budget, and only the
+    # requests measured here are served below
     plain_service = []
+    t_plain = time.perf_counter()
     for g, p, d in reqs:
+        if plain_service and time.perf_counter() - t_plain > args.plain_budget_s:
+            break
         t = 0.0
         with eg.ResidentGame(eg.threshold_game(g, int(p[0]), d)) as r:
             _, st0 = r.solve()
@@ -325,6 +347,8 @@ def run_served(args):
             _, st = eg.solve(eg.threshold_game(g, int(p[k]), d))
             t += st.solve_ms
         plain_service.append(t)
+        progress(f"plain request {len(plain_service)}: n={g.num_nodes} K={len(p)} {t:.1f} ms")
+    reqs = reqs[:len(plain_service)]
     results = []
     for rate in [float(x) for x in args.rates.split(",")]:
         arrivals = np.cumsum(rng.exponential(1.0 / rate, size=len(reqs)))
@@ -338,8 +362,9 @@ def run_served(args):
                     time.sleep(delay)
                 qids.append(srv.submit(gids[i], p, d))
             for q in qids:
-                srv.wait(q, 3_600_000)
+                srv.wait(q, 600_000)
             st = srv.stats()
+        progress(f"rate {rate}: p50 {st['latency_p50_ms']:.1f} ms, p99 {st['latency_p99_ms']:.1f} ms")
         # the same arrivals served one game at a time
         fin, lat = 0.0, []
         for a, s in zip(arrivals, plain_service):

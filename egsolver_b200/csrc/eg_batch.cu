@@ -10,13 +10,15 @@
  * single contiguous row.
  *
  * Kernel: every CTA takes a game from a device queue (largest games first),
- * computes MG_k = sum_v max(0, p_k - d * min_w(v)) and the initial frontier
- * for all thresholds, then runs the lifting rounds of that game alone with
- * CTA barriers; its frontier bitmaps live in shared memory, so the push of
- * a predecessor is a shared-memory atomicOr.  The lift of vertex v for
- * threshold k is the reference's (reference src/dev_EG_alg.cu:84-109) on the
- * weights w * d - p_k.  No wait in this kernel spins: rounds end at
- * __syncthreads and games come from an atomic counter.
+ * computes MG_k = sum_v max(0, p_k - d * min_w(v)), then runs dense rounds
+ * of that game alone with CTA barriers: every vertex lifted at every
+ * threshold per round, eight independent credit gathers in flight per lane.
+ * Mean-payoff threshold games take thousands of rounds in which most
+ * vertices rise, so a frontier would hold nearly every vertex anyway.  The
+ * lift of vertex v for threshold k is the reference's (reference
+ * src/dev_EG_alg.cu:84-109) on the weights w * d - p_k.  No wait in this
+ * kernel spins: rounds end at __syncthreads and games come from an atomic
+ * counter.
  */
 #include "eg_batch.cuh"
 
@@ -44,44 +46,36 @@ using namespace eg;
 
 namespace {
 
-__device__ __forceinline__ int nth_bit(uint32_t w, int k)
-{
-    int pos = 0;
-#pragma unroll
-    for (int s = 16; s > 0; s >>= 1) {
-        const uint32_t low = w & ((1u << s) - 1u);
-        const int c = __popc(low);
-        if (k >= c) {
-            k -= c;
-            w >>= s;
-            pos += s;
-        } else {
-            w = low;
-        }
-    }
-    return pos;
-}
-
+/* OMINUS on 64-bit credits for the weight b = w * d - p (reference
+ * src/common.h:270-272); the difference is formed without overflow and only
+ * used when a is finite. */
 __device__ __forceinline__ long long ominus64(long long a, long long b, long long mg)
 {
     const long long t = (long long)INT64_MAX;
-    const long long x = a - b;
+    const long long x = (long long)((unsigned long long)a - (unsigned long long)b);
     return (a < t && x <= mg) ? (x > 0 ? x : 0) : t;
 }
 
-/* KP lanes per vertex (KP >= K, a power of two); lane k serves threshold k. */
+/* Edges of a vertex taken together per step of the lift loop: independent
+ * credit gathers in flight per lane. */
+constexpr int kBatchUnroll = 8;
+
+/* KP lanes per vertex (KP >= K, a power of two); lane k serves threshold k.
+ * Dense rounds: each round lifts every vertex of the game at every
+ * threshold in place (no frontier), and the game is solved after a round
+ * without a raise.  Every lift reads credits that are the round's start
+ * values or values raised since, all below the least fixed point, so this is
+ * a fair chaotic iteration of the same operator and the credits equal the
+ * worklist solver's. */
 template <int KP>
 __global__ void __launch_bounds__(1024) k_batch_solve(const __grid_constant__ BatchParams p)
 {
-    extern __shared__ uint32_t sm[];
     __shared__ int s_game;
-    __shared__ int s_ctr[2];
     __shared__ long long s_mg[KP];
     __shared__ int s_p[KP];
-    constexpr int NG = 32 / KP;
     const int tid = threadIdx.x, lane = tid & 31;
-    const int grp = lane / KP, gl = lane % KP;
-    const unsigned gmask = (KP == 32) ? 0xffffffffu : (((1u << KP) - 1u) << (grp * KP));
+    const int gl = lane % KP;
+    const int group = tid / KP, ngroups = blockDim.x / KP;
     const long long TOP = (long long)INT64_MAX;
     unsigned long long lifts = 0, edges = 0, ntop = 0;
     if (blockIdx.x == 0 && tid == 0) p.ctrl->t_start = globaltimer_ns();
@@ -99,28 +93,13 @@ __global__ void __launch_bounds__(1024) k_batch_solve(const __grid_constant__ Ba
         const int2 *E = gd.E;
         const unsigned char *owner = gd.owner;
         long long *F = gd.F - base * K; /* indexed by id * K + k with ids base-relative */
-        const int W = (n + 31) >> 5;
-        uint32_t *cur = sm, *nxt = sm + p.words_max;
         if (tid < KP) {
             s_p[tid] = gd.thr[tid < K ? tid : 0];
             s_mg[tid] = 0;
         }
-        if (tid < 2) s_ctr[tid] = 0;
-        for (int w = tid; w < W; w += blockDim.x) {
-            cur[w] = 0;
-            nxt[w] = 0;
-        }
+        for (long long i = tid; i < (long long)n * K; i += blockDim.x) gd.F[i] = 0;
         __syncthreads();
-        /* f = 0, MG per threshold, initial frontier (any threshold) */
-        for (int v = tid; v < n; v += blockDim.x) {
-            const long long gv = base + v;
-            for (int k = 0; k < K; k++) F[gv * K + k] = 0;
-            const long long lo = (long long)gd.minw[v] * d, hi = (long long)gd.maxw[v] * d;
-            const int own = owner[v];
-            bool act = false;
-            for (int k = 0; k < K; k++) act |= own ? (lo - s_p[k] < 0) : (hi - s_p[k] < 0);
-            if (act) atomicOr(&cur[v >> 5], 1u << (v & 31));
-        }
+        /* MG per threshold: sum_v max(0, p_k - d * min_w(v)) */
         for (int k = 0; k < K; k++) {
             long long s = 0;
             for (int v = tid; v < n; v += blockDim.x) {
@@ -138,64 +117,43 @@ __global__ void __launch_bounds__(1024) k_batch_solve(const __grid_constant__ Ba
         long long r = 0;
         int st = EG_OK;
         for (;;) {
-            if (tid == 0) s_ctr[(r + 1) & 1] = 0;
-            int any_new = 0;
-            for (;;) {
-                int w0 = 0;
-                if (lane == 0) w0 = atomicAdd(&s_ctr[r & 1], 1);
-                w0 = __shfl_sync(0xffffffffu, w0, 0);
-                if (w0 >= W) break;
-                uint32_t word = cur[w0];
-                __syncwarp();
-                if (lane == 0 && word) cur[w0] = 0;
-                while (word) {
-                    const int c = __popc(word);
-                    if (grp < c) {
-                        const int v = (w0 << 5) + nth_bit(word, grp);
-                        const long long gv = base + v;
-                        const int own = owner[v];
-                        long long acc = own ? 0 : TOP;
-                        const int eb = P[v], ee = P[v + 1];
-                        for (int e = eb; e < ee; e++) {
-                            const int2 q = __ldg(E + e);
-                            if (valid) {
-                                const long long val = ominus64(F[(long long)q.x * K + gl], (long long)q.y * d - pk, mgk);
-                                acc = own ? (val > acc ? val : acc) : (val < acc ? val : acc);
-                            }
-                        }
-                        bool ch = false;
-                        if (valid) {
-                            const long long old = F[gv * K + gl];
-                            if (old < acc) {
-                                F[gv * K + gl] = acc;
-                                ch = true;
-                            }
-                        }
-                        const unsigned chm = __ballot_sync(gmask, ch) & gmask;
-                        if (chm) {
-                            const int cb = gd.CP[v], ce = gd.CP[v + 1];
-                            for (int j = cb + gl; j < ce; j += KP) {
-                                const int pr = (int)(gd.CS[j] - base);
-                                const uint32_t bit = 1u << (pr & 31);
-                                if (!(atomicOr(&nxt[pr >> 5], bit) & bit)) any_new = 1;
-                            }
-                        }
-                        if (gl == 0) {
-                            lifts++;
-                            edges += (unsigned long long)(ee - eb) * (unsigned long long)K;
+            int raised = 0;
+            for (int v = group; v < n; v += ngroups) {
+                const long long gv = base + v;
+                const int own = owner[v];
+                long long acc = own ? 0 : TOP;
+                const int eb = P[v], ee = P[v + 1];
+                for (int e = eb; e < ee; e += kBatchUnroll) {
+                    int2 q[kBatchUnroll];
+                    long long f[kBatchUnroll];
+#pragma unroll
+                    for (int j = 0; j < kBatchUnroll; j++)
+                        if (e + j < ee) q[j] = __ldg(E + e + j);
+#pragma unroll
+                    for (int j = 0; j < kBatchUnroll; j++)
+                        f[j] = (valid && e + j < ee) ? F[(long long)q[j].x * K + gl] : 0;
+#pragma unroll
+                    for (int j = 0; j < kBatchUnroll; j++) {
+                        if (valid && e + j < ee) {
+                            const long long val = ominus64(f[j], (long long)q[j].y * d - pk, mgk);
+                            acc = own ? (val > acc ? val : acc) : (val < acc ? val : acc);
                         }
                     }
-                    if (c <= NG) {
-                        word = 0;
-                    } else {
-                        const int last = nth_bit(word, NG - 1);
-                        word &= ~((2u << last) - 1u);
+                }
+                if (valid) {
+                    const long long old = F[gv * K + gl];
+                    if (old < acc) {
+                        F[gv * K + gl] = acc;
+                        raised = 1;
                     }
+                }
+                if (gl == 0) {
+                    lifts++;
+                    edges += (unsigned long long)(ee - eb) * (unsigned long long)K;
                 }
             }
             r++;
-            const int cont = __syncthreads_or(any_new);
-            if (!cont) break;
+            if (!__syncthreads_or(raised)) break;
             if (p.max_rounds >= 0 && r >= p.max_rounds) {
                 st = EG_ERR_LOOPCAP;
                 break;
@@ -206,9 +164,6 @@ __global__ void __launch_bounds__(1024) k_batch_solve(const __grid_constant__ Ba
                 st = EG_ERR_TIMEOUT;
                 break;
             }
-            uint32_t *t = cur;
-            cur = nxt;
-            nxt = t;
         }
         /* TOP count of this game (all thresholds) */
         for (long long i = tid; i < (long long)n * K; i += blockDim.x) ntop += (gd.F[i] == TOP);
@@ -395,11 +350,9 @@ batch_kernel_t kernel_for(int kp)
 eg_status launch_batch(const BatchParams &p, int KP, int block, int num_sms, cudaStream_t st, int *grid_out)
 {
     batch_kernel_t fn = kernel_for(KP);
-    const size_t smem = sizeof(uint32_t) * 2 * (size_t)p.words_max;
-    cudaError_t e = cudaFuncSetAttribute((const void *)fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e != cudaSuccess) return eg_set_error(EG_ERR_CUDA, "shared memory request failed: %s", cudaGetErrorString(e));
+    const size_t smem = 0; /* dense rounds keep no frontier */
     int per_sm = 0;
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void *)fn, block, smem);
+    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void *)fn, block, smem);
     if (e != cudaSuccess || per_sm < 1)
         return eg_set_error(EG_ERR_CUDA, "batch kernel does not fit (block %d, %zu B shared)", block, smem);
     int grid = num_sms * per_sm;
