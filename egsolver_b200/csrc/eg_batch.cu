@@ -118,11 +118,25 @@ __global__ void __launch_bounds__(1024) k_batch_solve(const __grid_constant__ Ba
         int st = EG_OK;
         for (;;) {
             int raised = 0;
+            /* the next vertex's row and owner load while this one is lifted */
+            int eb = 0, ee = 0, own = 0;
+            if (group < n) {
+                eb = P[group];
+                ee = P[group + 1];
+                own = owner[group];
+            }
             for (int v = group; v < n; v += ngroups) {
                 const long long gv = base + v;
-                const int own = owner[v];
+                const int vn = v + ngroups;
+                int ebn = 0, een = 0, ownn = 0;
+                if (vn < n) {
+                    ebn = P[vn];
+                    een = P[vn + 1];
+                    ownn = owner[vn];
+                }
+                /* only this lane writes F[v][k] in a round: read it early */
+                const long long old = valid ? F[gv * K + gl] : 0;
                 long long acc = own ? 0 : TOP;
-                const int eb = P[v], ee = P[v + 1];
                 for (int e = eb; e < ee; e += kBatchUnroll) {
                     int2 q[kBatchUnroll];
                     long long f[kBatchUnroll];
@@ -140,17 +154,17 @@ __global__ void __launch_bounds__(1024) k_batch_solve(const __grid_constant__ Ba
                         }
                     }
                 }
-                if (valid) {
-                    const long long old = F[gv * K + gl];
-                    if (old < acc) {
-                        F[gv * K + gl] = acc;
-                        raised = 1;
-                    }
+                if (valid && old < acc) {
+                    F[gv * K + gl] = acc;
+                    raised = 1;
                 }
                 if (gl == 0) {
                     lifts++;
                     edges += (unsigned long long)(ee - eb) * (unsigned long long)K;
                 }
+                eb = ebn;
+                ee = een;
+                own = ownn;
             }
             r++;
             if (!__syncthreads_or(raised)) break;
@@ -476,7 +490,7 @@ extern "C" eg_status eg_batch_create(const eg_game *games, int32_t num_games, co
     b->total_nodes = tn;
     b->total_edges = tm;
     b->words_max = (nmax + 31) / 32;
-    b->block = opts->block ? opts->block : 256;
+    b->block = opts->block ? opts->block : 1024;
     b->max_rounds = opts->max_rounds;
     b->timeout_ms = opts->timeout_ms;
     b->use_graph = opts->use_graph != 0;
@@ -753,7 +767,7 @@ extern "C" eg_status eg_batch_tune(eg_batch *b, int32_t *block_out)
 {
     if (!b) return eg_set_error(EG_ERR_INVALID, "batch is NULL");
     if (!b->thresholds_set) return eg_set_error(EG_ERR_INVALID, "thresholds not set");
-    const int cands[] = {128, 256, 512, 1024};
+    const int cands[] = {256, 512, 1024};
     const long long keep_cap = b->max_rounds;
     const bool keep_graph = b->use_graph;
     b->use_graph = false;

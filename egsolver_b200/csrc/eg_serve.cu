@@ -473,7 +473,7 @@ extern "C" eg_status eg_serve_create(const eg_serve_opts *opts, eg_server **out)
     }
     if (s->o.max_inflight <= 0) s->o.max_inflight = 1024;
     if (s->o.streams <= 0) s->o.streams = 4;
-    if (s->o.block <= 0) s->o.block = 256;
+    if (s->o.block <= 0) s->o.block = 1024;
     if (s->o.hbm_reserve_bytes <= 0) s->o.hbm_reserve_bytes = 1ll << 30;
     if (s->o.large_ctas <= 0) s->o.large_ctas = 148;
     if (s->o.max_rounds == 0) s->o.max_rounds = -1;

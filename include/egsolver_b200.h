@@ -258,7 +258,7 @@ typedef struct eg_batch eg_batch;
 typedef struct eg_batch_opts {
     int32_t thresholds;          /* K thresholds per game, 1..EG_BATCH_MAX_K        */
     int32_t scale;               /* d >= 1: threshold p turns w into w*d - p        */
-    int32_t block;               /* threads per CTA (128..1024); 0 = autotuned      */
+    int32_t block;               /* threads per CTA (64..1024); 0 = 1024 (eg_batch_tune picks one) */
     int32_t device;
     int64_t max_rounds;          /* per game; < 0: no cap                           */
     double  timeout_ms;          /* per launch; <= 0: none                          */

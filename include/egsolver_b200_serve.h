@@ -31,7 +31,7 @@ typedef struct eg_serve_opts {
     int32_t device;
     int32_t max_inflight;        /* queries admitted at once (0 = 1024)              */
     int32_t streams;             /* micro-batches in flight at once (0 = 4)          */
-    int32_t block;               /* threads per CTA of the batched kernel (0 = 256)  */
+    int32_t block;               /* threads per CTA of the batched kernel (0 = 1024) */
     int64_t hbm_reserve_bytes;   /* device memory admission leaves free (0 = 1 GiB)  */
     int64_t max_rounds;          /* per query; < 0: no cap                           */
     int32_t large_ctas;          /* CTAs of the grid solver for large games (0: 148)  */
