@@ -4,10 +4,13 @@
 
 WORKLOAD is cfg2 (n = 2^20 sparse game) or cfg3 (2000-vertex clique);
 WHICH is "reference" (the reference's EG_cpu_solver compiled unmodified,
-oracle/_ref/libegref.so, int32 credits) or "port" (the int64 restatement in
-oracle/eg_oracle.c).  The solve is a serial worklist run to the least fixed
-point; on cfg2 it takes hours, which is why its result is committed as a
-digest rather than recomputed by the tests.
+oracle/_ref/libegref.so, int32 credits), "port" (the int64 worklist
+restatement in oracle/eg_oracle.c), or "eg0-omp" (the restatement of the
+reference's EG0 Jacobi sweeps with its thread-safety defects fixed, int32
+credits, all host cores).  Every schedule reaches the same least fixed
+point.  The serial worklist takes hours on cfg2 and the Jacobi sweeps tens of
+minutes on eight cores, which is why the result is committed as a digest
+rather than recomputed by the tests.
 
 OUT.json records: the SHA-256 of the credits as little-endian int64 in
 vertex order with TOP written as INT64_MAX, the number of TOP vertices, the
@@ -18,6 +21,7 @@ from __future__ import annotations
 
 import hashlib
 import json
+import os
 import sys
 import time
 from pathlib import Path
@@ -48,6 +52,13 @@ def main(workload: str, which: str, out: str) -> None:
         f = f32.astype(np.int64)
         f[f32 == O.TOP32] = TOP64
         info = {"pops": st["processed"], "mg": st["mg"], "reference_seconds": st["seconds"]}
+    elif which == "eg0-omp":
+        threads = os.cpu_count() or 1
+        f32, st = O.eg0_solve(game, threads=threads)
+        f = f32.astype(np.int64)
+        f[f32 == O.TOP32] = TOP64
+        info = {"sweeps": st["loops"], "mg": st["mg"], "edges": st["edges"], "finished": st["finished"],
+                "threads": threads}
     else:
         f, st = O.eg_solve(game, bits=64)
         info = {"pops": st["processed"], "mg": st["mg"], "edges": st["edges"], "finished": st["finished"]}
