@@ -241,6 +241,20 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+def reduce_over_ranks(dist, dev_ms: float, edges: float, device: str) -> tuple[float, float]:
+    """Whole-job figures of N replicas: the slowest rank's device time and
+    the edges of all ranks (dist None: this process alone)."""
+    if dist is None:
+        return float(dev_ms), float(edges)
+    import torch
+
+    t = torch.tensor([float(dev_ms)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    e = torch.tensor([float(edges)], dtype=torch.float64, device=device)
+    dist.all_reduce(e, op=dist.ReduceOp.SUM)
+    return float(t.item()), float(e.item())
+
+
 def progress(msg: str) -> None:
     """A progress line on stderr (the JSON result line stays alone on stdout)."""
     print(f"[bench] {msg}", file=sys.stderr, flush=True)
@@ -452,14 +466,7 @@ def main():
     # correctness guard on the last timed solve: a fixed point of the lifting operator
     credits = res.credits(64)
     res.free()
-    if dist:
-        t = torch.tensor([dev_ms], dtype=torch.float64, device=f"cuda:{local}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e = torch.tensor([float(edges)], dtype=torch.float64, device=f"cuda:{local}")
-        dist.all_reduce(e, op=dist.ReduceOp.SUM)
-        dev_ms_max, edges_all = float(t.item()), float(e.item())
-    else:
-        dev_ms_max, edges_all = dev_ms, float(edges)
+    dev_ms_max, edges_all = reduce_over_ranks(dist, dev_ms, edges, f"cuda:{local}")
     value = edges_all / (dev_ms_max / 1e3) / 1e9
 
     # e2e through the one-call API with pinned host buffers
