@@ -144,7 +144,7 @@ def make_opts(credit_bits: int = 64, variant: int = VARIANT_AUTO, max_rounds: in
               keep_layout: bool = False, cancel: Optional["CancelFlag"] = None, grid_ctas: int = 0,
               task_edges: int = 0, schedule: int = 0, profile: bool = False, ctas_per_sm: int = 0,
               direction: int = 0, dense_permille: int = 0, sparse_permille: int = 0, narrow: bool = False,
-              wide_pairs: bool = False, dense_depth: int = 0) -> _ffi.EgOpts:
+              wide_pairs: bool = False, dense_depth: int = 0, dense_sweeps: int = 0) -> _ffi.EgOpts:
     o = _ffi.EgOpts()
     lib().eg_opts_default(C.byref(o))
     o.credit_bits = credit_bits
@@ -167,6 +167,7 @@ def make_opts(credit_bits: int = 64, variant: int = VARIANT_AUTO, max_rounds: in
     o.narrow = 1 if narrow else 0
     o.wide_pairs = 1 if wide_pairs else 0
     o.dense_depth = dense_depth
+    o.dense_sweeps = dense_sweeps
     o.cancel = cancel.ptr if cancel is not None else None
     return o
 

@@ -59,6 +59,7 @@ class EgOpts(C.Structure):
         ("narrow", C.c_int32),
         ("wide_pairs", C.c_int32),
         ("dense_depth", C.c_int32),
+        ("dense_sweeps", C.c_int32),
     ]
 
 

@@ -199,6 +199,8 @@ static eg_status check_lanes(const eg_opts *o)
         return eg_set_error(EG_ERR_INVALID, "credit_bits must be 32 or 64 (got %d)", o->credit_bits);
     if (o && (o->direction < EG_DIRECTION_SWITCH || o->direction > EG_DIRECTION_DENSE))
         return eg_set_error(EG_ERR_INVALID, "unknown direction %d", o->direction);
+    if (o && (o->dense_sweeps < 0 || o->dense_sweeps > 2))
+        return eg_set_error(EG_ERR_INVALID, "dense_sweeps must be 0, 1 or 2 (got %d)", o->dense_sweeps);
     if (o && (o->dense_depth < 0 || o->dense_depth > 2))
         return eg_set_error(EG_ERR_INVALID, "dense_depth must be 0, 1 or 2 (got %d)", o->dense_depth);
     if (o && (o->dense_permille < 0 || o->dense_permille > 1000 || o->sparse_permille < 0 || o->sparse_permille > 1000))
@@ -305,8 +307,8 @@ static eg_status dgame_alloc(const eg_game *game, const eg_opts *opts, eg_dgame 
     if (s == EG_OK) s = dalloc(g, &g->d_PM, (size_t)(g->m_pad_cap / 2 + 64));
     if (s == EG_OK) s = dalloc(g, &g->d_CB, (size_t)(g->m_pad_cap / 64 + 4));
     if (s == EG_OK) s = dalloc(g, &g->d_merr, 1);
-    if (s == EG_OK) s = dalloc(g, &g->d_drem, (size_t)g->n_pad_cap);
-    if (s == EG_OK) s = dalloc(g, (int64_t **)&g->d_dacc, (size_t)g->n_pad_cap);
+    if (s == EG_OK) s = dalloc(g, &g->d_drem, 2 * (size_t)g->n_pad_cap); /* one bank per sweep */
+    if (s == EG_OK) s = dalloc(g, (int64_t **)&g->d_dacc, 2 * (size_t)g->n_pad_cap);
     if (s == EG_OK) s = dalloc(g, &g->d_E8, (size_t)(g->m_pad_cap / 2 + 64));
     if (s != EG_OK) {
         eg_dgame_free(g);
@@ -589,6 +591,7 @@ extern "C" eg_status eg_dgame_solve(eg_dgame *g, const eg_opts *opts_in, eg_stat
     if (kinds) {
         /* one slice of the pair stream per warp of the dense grid */
         p.dense_depth = opts->dense_depth == 1 ? 1 : 2;
+        p.dense_sweeps = opts->dense_sweeps == 2 ? 2 : 1;
         EG_TRY(dense_grid(bits, p.dense_depth, opts->grid_ctas, &dgrid));
         const long long warps = (long long)dgrid * 16;
         const long long per = (g->npairs + warps - 1) / warps;

@@ -123,7 +123,7 @@ void build_pair_meta(const int *P, int n_pad, int npairs, const ClassTable &ct, 
 /* ------------------------------------------------------------------ */
 
 template <class T>
-__global__ void k_dense_setup(const int *P, int n_pad, const uint16_t *PM, int slice, T *dacc, int *drem)
+__global__ void k_dense_setup(const int *P, int n_pad, const uint16_t *PM, int slice, int banks, T *dacc, int *drem)
 {
     const int u = blockIdx.x * blockDim.x + threadIdx.x;
     if (u >= n_pad) return;
@@ -131,8 +131,10 @@ __global__ void k_dense_setup(const int *P, int n_pad, const uint16_t *PM, int s
     if (e <= b) return;
     const int nrep = (e - 1) / slice - b / slice + 1;
     if (nrep > 1) {
-        drem[u] = nrep;
-        dacc[u] = (PM[b] & PM_OWNER) ? (T)0 : credit_traits<T>::top;
+        for (int k = 0; k < banks; k++) {
+            drem[(size_t)k * n_pad + u] = nrep;
+            dacc[(size_t)k * n_pad + u] = (PM[b] & PM_OWNER) ? (T)0 : credit_traits<T>::top;
+        }
     }
 }
 
@@ -140,9 +142,11 @@ void launch_dense_setup(const LiftParams &p, int credit_bits, cudaStream_t st)
 {
     const int grid = (p.n_pad + kMetaBlock - 1) / kMetaBlock;
     if (credit_bits == 32)
-        k_dense_setup<int32_t><<<grid, kMetaBlock, 0, st>>>(p.P, p.n_pad, p.PM, p.slice, (int32_t *)p.dacc, p.drem);
+        k_dense_setup<int32_t><<<grid, kMetaBlock, 0, st>>>(p.P, p.n_pad, p.PM, p.slice, p.dense_sweeps,
+                                                            (int32_t *)p.dacc, p.drem);
     else
-        k_dense_setup<int64_t><<<grid, kMetaBlock, 0, st>>>(p.P, p.n_pad, p.PM, p.slice, (int64_t *)p.dacc, p.drem);
+        k_dense_setup<int64_t><<<grid, kMetaBlock, 0, st>>>(p.P, p.n_pad, p.PM, p.slice, p.dense_sweeps,
+                                                            (int64_t *)p.dacc, p.drem);
 }
 
 /* ------------------------------------------------------------------ */
@@ -175,19 +179,24 @@ __device__ __forceinline__ int32_t ominus_fast(int32_t a, int32_t w, int32_t mg)
 }
 
 /* A slice's partial value v (actual, not negated) of cut vertex u; the
- * slice that reports last raises the credit.  Returns whether it rose. */
+ * slice that reports last raises the credit.  Returns whether it rose.
+ * Each sweep of a round has its own accumulator bank: a warp may start its
+ * next sweep before a slower warp has reported the same vertex for this
+ * one, and mixing their reports would combine part of the edges only. */
 template <class T>
-__device__ __forceinline__ bool dense_report(const LiftParams &p, T *F, int u, bool own, T v, unsigned &changes)
+__device__ __forceinline__ bool dense_report(const LiftParams &p, T *F, int u, bool own, T v, unsigned &changes,
+                                             int bank)
 {
-    T *acc = (T *)p.dacc;
+    T *acc = (T *)p.dacc + (size_t)bank * p.n_pad;
+    int *rem = p.drem + (size_t)bank * p.n_pad;
     if (own) atomic_combine<1>(acc + u, v);
     else atomic_combine<0>(acc + u, v);
     __threadfence();
-    if (atomicSub(p.drem + u, 1) != 1) return false;
+    if (atomicSub(rem + u, 1) != 1) return false;
     __threadfence();
     const T r = atomic_swap(acc + u, own ? (T)0 : credit_traits<T>::top);
     const int b = __ldg(p.P + u) >> 1, e = __ldg(p.P + u + 1) >> 1;
-    p.drem[u] = (e - 1) / p.slice - b / p.slice + 1; /* ready for the next round */
+    rem[u] = (e - 1) / p.slice - b / p.slice + 1; /* ready for the next round */
     const T old = ld_credit(F + u);
     if (old < r) {
         st_credit(F + u, r);
@@ -295,7 +304,7 @@ struct Carry {
 template <class T, bool FAST, bool PACKED>
 __device__ __forceinline__ void compute_chunk(const LiftParams &p, T *F, uint32_t *ch, bool rec, const Chunk &k, T fa,
                                               T fb, T old, int lane, uint32_t le_mask, Carry<T> &cr,
-                                              unsigned &changes)
+                                              unsigned &changes, int bank)
 {
     constexpr T top = credit_traits<T>::top;
     const int u = k.base + (int)(k.md & PM_OFF);
@@ -330,7 +339,7 @@ __device__ __forceinline__ void compute_chunk(const LiftParams &p, T *F, uint32_
     if (k.in && end) {
         const T v = own ? -x : x;
         if (head == 0 && cr.cut) {
-            raise = dense_report<T>(p, F, u, own, v, changes);
+            raise = dense_report<T>(p, F, u, own, v, changes, bank);
         } else if (old < v) {
             st_credit(F + u, v);
             changes++;
@@ -354,7 +363,7 @@ __device__ __forceinline__ void compute_chunk(const LiftParams &p, T *F, uint32_
  * flight while a chunk is reduced (more registers: two CTAs per SM). */
 template <class T, bool FAST, bool PACKED, int DEPTH>
 __device__ __forceinline__ void dense_slice(const LiftParams &p, T *F, uint32_t *ch, bool rec, int s0, int s1,
-                                            int lane, unsigned &changes)
+                                            int lane, unsigned &changes, int bank)
 {
     if (s0 >= s1) return;
     const uint32_t le_mask = 0xffffffffu >> (31 - lane);
@@ -372,7 +381,7 @@ __device__ __forceinline__ void dense_slice(const LiftParams &p, T *F, uint32_t 
             load_chunk<PACKED>(p, c0 + 32, s1, lane, k1);
             T fa, fb, old;
             gather_chunk<T, PACKED>(p, F, k0, fa, fb, old);
-            compute_chunk<T, FAST, PACKED>(p, F, ch, rec, k0, fa, fb, old, lane, le_mask, cr, changes);
+            compute_chunk<T, FAST, PACKED>(p, F, ch, rec, k0, fa, fb, old, lane, le_mask, cr, changes, bank);
             k0 = k1;
         }
     } else {
@@ -384,7 +393,7 @@ __device__ __forceinline__ void dense_slice(const LiftParams &p, T *F, uint32_t 
             load_chunk<PACKED>(p, c0 + 64, s1, lane, k2);
             T fa1, fb1, old1;
             gather_chunk<T, PACKED>(p, F, k1, fa1, fb1, old1);
-            compute_chunk<T, FAST, PACKED>(p, F, ch, rec, k0, fa0, fb0, old0, lane, le_mask, cr, changes);
+            compute_chunk<T, FAST, PACKED>(p, F, ch, rec, k0, fa0, fb0, old0, lane, le_mask, cr, changes, bank);
             k0 = k1;
             k1 = k2;
             fa0 = fa1;
@@ -396,7 +405,7 @@ __device__ __forceinline__ void dense_slice(const LiftParams &p, T *F, uint32_t 
     const int cu = __shfl_sync(0xffffffffu, cr.u_last, 31);
     const bool cown = __shfl_sync(0xffffffffu, (int)cr.own_last, 31) != 0;
     if (cr.on && lane == 0) {
-        const bool r = dense_report<T>(p, F, cu, cown, cown ? -cr.val : cr.val, changes);
+        const bool r = dense_report<T>(p, F, cu, cown, cown ? -cr.val : cr.val, changes, bank);
         if (rec && r) atomicOr(ch + (cu >> 5), 1u << (cu & 31));
     }
 }
@@ -436,7 +445,10 @@ __global__ void __launch_bounds__(DENSE_BLOCK, DEPTH == 1 ? 3 : 2) k_lift_dense(
         }
         const unsigned changes0 = changes;
         const unsigned long long t0 = p.profile ? globaltimer_ns() : 0ull;
-        dense_slice<T, FAST, PACKED, DEPTH>(p, F, ch, kind == ROUND_RECORD, s0, s1, lane, changes);
+        /* dense_sweeps sweeps of the slice per grid barrier; a round
+         * without a raise in any of them ends the solve */
+        for (int sw = 0; sw < p.dense_sweeps; sw++)
+            dense_slice<T, FAST, PACKED, DEPTH>(p, F, ch, kind == ROUND_RECORD, s0, s1, lane, changes, sw);
         if (p.profile && lane == 0) {
             const unsigned long long dt = globaltimer_ns() - t0;
             atomicAdd(&s_busy, dt);

@@ -61,6 +61,7 @@ struct LiftParams {
     int wbits, wbias;          /* packed edge: (succ << wbits) | (w + wbias)       */
     int fast32;                /* 32-bit credits whose differences fit 32 bits     */
     int dense_depth;           /* chunks in flight per warp: 1 (3 CTAs per SM) or 2 */
+    int dense_sweeps;          /* sweeps of every slice per grid barrier: 1 or 2    */
 };
 
 /* Round kinds, as Ctrl::next_mode holds them between rounds and launches. */

@@ -132,6 +132,8 @@ typedef struct eg_opts {
                                     even when successor and weight fit 32 bits        */
     int32_t dense_depth;         /* chunks in flight per warp in dense rounds: 1 (three
                                     CTAs per SM) or 2 (two CTAs per SM); 0: 2         */
+    int32_t dense_sweeps;        /* sweeps of the edge stream per grid barrier in dense
+                                    rounds: 1 or 2; 0: 1                              */
 } eg_opts;
 
 typedef struct eg_stats {

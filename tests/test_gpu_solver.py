@@ -136,7 +136,8 @@ def test_round_kinds_give_identical_credits(cfg2_2e14, d, bits):
 # (narrow, when MG + max|w| fits) 32-bit credits with warp reductions; 8-byte
 # or 16-byte edge pairs.
 DENSE_PATHS = [dict(), dict(wide_pairs=True), dict(narrow=True), dict(narrow=True, wide_pairs=True),
-               dict(dense_depth=1), dict(dense_depth=1, narrow=True, wide_pairs=True)]
+               dict(dense_depth=1), dict(dense_depth=1, narrow=True, wide_pairs=True), dict(dense_sweeps=2),
+               dict(dense_sweeps=2, narrow=True, dense_depth=1)]
 
 
 @pytest.mark.parametrize("d", DENSE_PATHS, ids=lambda d: vid(d) or "default")
