@@ -153,7 +153,7 @@ def measured_peak():
 
 
 def dense_round_bytes(game, credit_bytes: int) -> int:
-    """Algorithmic bytes of one dense round: per edge pair (two out-edges,
+    """Algorithmic bytes of one dense sweep: per edge pair (two out-edges,
     odd degrees padded) 16 B of {succ, w} x 2 and 2 B of metadata, 4 B per
     32-pair chunk; per out-edge the successor's credit S; per vertex its own
     credit S.  (Credit writes, S per raise, are added from the raise count.)"""
@@ -533,7 +533,7 @@ def main():
                     traffic = d["dram_bytes_per_round"] * d_rounds / d_launch
             except (ValueError, KeyError):
                 traffic = None
-        extra = {"launches": d_launch, "rounds_per_launch": d_rounds / d_launch,
+        extra = {"launches": d_launch, "sweeps_per_launch": d_rounds / d_launch,
                  "ms_per_launch": d_ms / d_launch, "bytes_per_round": dense_round_bytes(game, S)}
     else:
         per_launch = lift_traffic_bytes(last, S)

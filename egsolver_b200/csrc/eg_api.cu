@@ -591,7 +591,7 @@ extern "C" eg_status eg_dgame_solve(eg_dgame *g, const eg_opts *opts_in, eg_stat
     if (kinds) {
         /* one slice of the pair stream per warp of the dense grid */
         p.dense_depth = opts->dense_depth == 1 ? 1 : 2;
-        p.dense_sweeps = opts->dense_sweeps == 2 ? 2 : 1;
+        p.dense_sweeps = opts->dense_sweeps == 1 ? 1 : 2;
         EG_TRY(dense_grid(bits, p.dense_depth, opts->grid_ctas, &dgrid));
         const long long warps = (long long)dgrid * 16;
         const long long per = (g->npairs + warps - 1) / warps;

@@ -471,7 +471,7 @@ __global__ void __launch_bounds__(DENSE_BLOCK, DEPTH == 1 ? 3 : 2) k_lift_dense(
         const bool ok = grid_barrier(c, p.wait_limit_ns, [&]() {
             c->flag[round & 1] = 0;
             c->rounds = round + 1;
-            c->dense_rounds++;
+            c->dense_rounds += p.dense_sweeps; /* sweeps over every vertex */
             if (p.profile) {
                 c->t_heavy += c->round_max[round & 1]; /* the slowest slice of the round */
                 c->round_max[round & 1] = 0ull;

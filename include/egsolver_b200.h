@@ -133,7 +133,7 @@ typedef struct eg_opts {
     int32_t dense_depth;         /* chunks in flight per warp in dense rounds: 1 (three
                                     CTAs per SM) or 2 (two CTAs per SM); 0: 2         */
     int32_t dense_sweeps;        /* sweeps of the edge stream per grid barrier in dense
-                                    rounds: 1 or 2; 0: 1                              */
+                                    rounds: 1 or 2; 0: 2                              */
 } eg_opts;
 
 typedef struct eg_stats {
@@ -151,7 +151,8 @@ typedef struct eg_stats {
     int64_t changes;             /* lifts that raised a credit                        */
     int64_t pushes;              /* predecessor entries scanned after those raises    */
     int32_t grid, block;         /* launch shape of the lifting kernel                */
-    int32_t dense_rounds;        /* rounds that lifted every vertex (no frontier)     */
+    int32_t dense_rounds;        /* sweeps that lifted every vertex (no frontier); a
+                                    dense round is dense_sweeps sweeps               */
     int32_t dense_launches;      /* launches of the dense-round kernel                */
     /* with opts.profile, in nanoseconds.  Frontier rounds only: mean time per
      * warp and round in heavy tasks, in word classes, and waiting at the round

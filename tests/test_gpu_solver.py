@@ -123,13 +123,14 @@ def test_round_kinds_give_identical_credits(cfg2_2e14, d, bits):
     else:
         np.testing.assert_array_equal(f, ref)
     assert st.grid > 1  # the grid kernel, not the one-CTA one
+    sweeps = 2  # default sweeps per dense round; dense_rounds counts sweeps
     if d["direction"] == eg.DIRECTION_SPARSE:
         assert st.dense_rounds == 0
     elif d["direction"] == eg.DIRECTION_DENSE:
-        assert st.dense_rounds == st.rounds
+        assert st.dense_rounds == sweeps * st.rounds
     elif d.get("sparse_permille") == 1000:
         # frontier, dense, recording dense, seed + frontier, ...
-        assert st.rounds // 3 <= st.dense_rounds < st.rounds
+        assert st.rounds // 3 <= st.dense_rounds // sweeps < st.rounds
 
 
 # Data paths of the dense rounds: 64-bit credits with a shuffle scan, or
