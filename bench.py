@@ -530,11 +530,11 @@ def main():
             try:
                 d = json.loads(tf.read_text())
                 if d.get("workload") == cfg["workload"] and d.get("n") == game.num_nodes:
-                    traffic = d["dram_bytes_per_round"] * d_rounds / d_launch
+                    traffic = d["dram_bytes_per_sweep"] * d_rounds / d_launch
             except (ValueError, KeyError):
                 traffic = None
         extra = {"launches": d_launch, "sweeps_per_launch": d_rounds / d_launch,
-                 "ms_per_launch": d_ms / d_launch, "bytes_per_round": dense_round_bytes(game, S)}
+                 "ms_per_launch": d_ms / d_launch, "bytes_per_sweep": dense_round_bytes(game, S)}
     else:
         per_launch = lift_traffic_bytes(last, S)
         achieved = per_launch / (last.lift_ms / 1e3) / 1e9
