@@ -9,7 +9,8 @@ successors uniform without self-loops or duplicates, weights uniform in
 [-1000, 1000], 64-bit credits; seeded (seed 0xE6 + 2), synthetic.
 
 A step is one complete solve from f = 0: transpose and renumbering,
-initial frontier, the persistent lifting kernel until the least fixed point.
+initial frontier, the persistent lifting kernels (frontier rounds, then
+dense rounds over every vertex) until the least fixed point.
   value  GTEPS = out-edges scanned by lifts / device time of the solve, with
          the game resident in HBM; device time from CUDA events on the
          solver's stream; L2 flushed (256 MB write) before every step
@@ -30,6 +31,14 @@ single-game solve does not shard); value = edges of all ranks / max time.
 
 --impl reference times the reference CPU solver alone (rank 0), each step a
 bounded sample of the same workload.
+
+--workload cfg4 (batched): the first --games games of the seeded 4096-game
+stream at K = 8 mean-payoff thresholds in one persistent launch, against
+one plain solve per (game, threshold) on a seeded sample.  --workload cfg5
+(served): the seeded request stream (n up to --n-max) through the serving
+loop at each --rates arrival rate, against the same arrivals served one at
+a time with measured plain service times.  Both cut their plain-path
+measurement after --plain-budget-s seconds.
 """
 from __future__ import annotations
 
