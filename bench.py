@@ -207,6 +207,21 @@ def cpu_sample(game, seconds: float, kind_pref: str = "reference"):
     return edges / secs / 1e9, edges, secs, P, "reference" if use_ref else "port"
 
 
+def cpu_sample_omp(game, seconds: float):
+    """Times the reference's own OpenMP EG0 (Jacobi sweeps, cpu_solver.c
+    EG0_cpu_solver, compiled unmodified) on all host cores for its first S
+    sweeps of `game`; every sweep scans all m edges.  Returns (gteps, S,
+    secs, threads)."""
+    from oracle import oracle as O
+
+    threads = os.cpu_count() or 1
+    S = 4
+    _, st = O.ref_cpu_solve(game, "eg0", threads=threads, max_loop_=S)
+    S = max(S, int(S * seconds / max(st["seconds"], 1e-3)))
+    _, st = O.ref_cpu_solve(game, "eg0", threads=threads, max_loop_=S)
+    return game.num_edges * S / st["seconds"] / 1e9, S, st["seconds"], threads
+
+
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -235,9 +250,10 @@ def run_reference(args):
         O.eg_solve(game, bits=32, max_loop_=P)
         return time.perf_counter() - t
 
-    for _ in range(args.warmup):
-        step()
-    times = [step() for _ in range(args.steps)]
+    with stdout_to_stderr():
+        for _ in range(args.warmup):
+            step()
+        times = [step() for _ in range(args.steps)]
     total = sum(times)
     value = edges * args.steps / total / 1e9
     kind = "reference" if use_ref else "port"
@@ -250,6 +266,23 @@ def run_reference(args):
                                        f"same game, {edges} edges relaxed per step"},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
+
+
+class stdout_to_stderr:
+    """Sends file descriptor 1 to stderr for the duration: the reference's C
+    solvers print progress lines, and stdout carries only the JSON line."""
+
+    def __enter__(self):
+        sys.stdout.flush()
+        self.saved = os.dup(1)
+        os.dup2(2, 1)
+        return self
+
+    def __exit__(self, *exc):
+        sys.stdout.flush()
+        os.dup2(self.saved, 1)
+        os.close(self.saved)
+        return False
 
 
 def reduce_over_ranks(dist, dev_ms: float, edges: float, device: str) -> tuple[float, float]:
@@ -555,12 +588,20 @@ def main():
                 "traffic": traffic, "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)",
                 "kernel": kernel, "algorithmic_bytes_per_launch": per_launch, **extra}
 
-    cpu = None
+    cpu = cpu_omp = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        g, ed, secs, P, kind = cpu_sample(game, args.cpu_sample_s)
+        with stdout_to_stderr():
+            g, ed, secs, P, kind = cpu_sample(game, args.cpu_sample_s)
         cpu = {"value": g, "unit": UNIT, "cores": 1, "kind": kind,
                "sample": f"first {P} worklist pops of EG_cpu_solver (reference --eg {P}) on the same game: "
                          f"{ed} edges in {secs:.2f} s"}
+        if kind == "reference":
+            with stdout_to_stderr():
+                og, S, osecs, th = cpu_sample_omp(game, args.cpu_sample_s / 2)
+            cpu_omp = {"value": og, "unit": UNIT, "cores": th, "kind": "reference",
+                       "sample": f"first {S} sweeps of the reference's OpenMP EG0_cpu_solver (--eg0, {th} threads; "
+                                 f"its shared inner index races, so only the timing is used): {S} x m edges in "
+                                 f"{osecs:.2f} s"}
 
     if rank == 0:
         if capped:
@@ -569,7 +610,8 @@ def main():
                 "warmup": args.warmup, "ms_per_step": dev_ms_max / args.steps, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": f"int{last.credit_bits}", "data": "synthetic",
                 "config": cfg,
-                "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(launches),
+                "roofline": roofline, "cpu_baseline": cpu, "cpu_baseline_omp": cpu_omp, "e2e": e2e,
+                "gpu_launches": int(launches),
                 "clocks": clocks,
                 "solve": {"rounds": last.rounds, "lifts": last.lifts, "edges": last.edges, "changes": last.changes,
                           "pushes": last.pushes, "num_top": last.num_top, "mg": last.mg,
