@@ -71,6 +71,8 @@ def parse():
     ap.add_argument("--games", type=int, default=64,
                     help="cfg4: the first G games of the 4096-game stream (same seeds)")
     ap.add_argument("--plain-sample", type=int, default=24, help="cfg4: (game, threshold) pairs timed on the plain path")
+    ap.add_argument("--batch-timeout-s", type=float, default=120.0,
+                    help="cfg4: device-side limit of one batched solve (games still running stop)")
     ap.add_argument("--plain-budget-s", type=float, default=45.0,
                     help="cfg4/cfg5: wall-clock budget of the plain-path measurements")
     ap.add_argument("--requests", type=int, default=16, help="cfg5: requests per arrival rate (at most)")
@@ -318,30 +320,33 @@ def run_batched(args):
     p, d = workloads.cfg4_thresholds(G)
     K = p.shape[1]
     t0 = time.perf_counter()
-    b = eg.Batch(games, thresholds=K, scale=d, use_graph=True)
+    b = eg.Batch(games, thresholds=K, scale=d, use_graph=True, timeout_ms=1e3 * args.batch_timeout_s)
     b.set_thresholds(p)
     setup_s = time.perf_counter() - t0
     progress(f"batch of {G} games uploaded in {setup_s:.1f} s")
     block = b.tune()
     progress(f"tuned: block {block}")
     for _ in range(args.warmup):
-        _, wst = b.solve()
-        progress(f"warm-up solve {wst.solve_ms:.1f} ms")
+        _, wst = b.solve(raise_on_error=False)
+        progress(f"warm-up solve {wst.solve_ms:.1f} ms, {wst.games_failed} game(s) stopped by the time limit")
     sampler = ClockSampler(0)
     times, stats = [], []
     for _ in range(args.steps):
-        _, st = b.solve()
+        _, st = b.solve(raise_on_error=False)
         times.append(st.solve_ms)
         stats.append(st)
-        progress(f"timed solve {st.solve_ms:.1f} ms")
+        progress(f"timed solve {st.solve_ms:.1f} ms, {st.games_failed} game(s) stopped by the time limit")
     clocks = sampler.stop()
     ms = sum(times) / len(times)
-    value = G / (ms / 1e3)
+    done = G - max(s.games_failed for s in stats)  # games solved to the fixed point in every step
+    value = done / (ms / 1e3)
     # parity spot check on the checker: fixed point of a few transformed games
     from oracle import oracle as O
 
     rng = np.random.default_rng(0)
     for g in rng.choice(G, size=min(8, G), replace=False):
+        if b.game_result(int(g))[1] != 0:
+            continue  # stopped by the time limit: its credits are lower bounds only
         cr = b.credits(int(g))
         for k in range(K):
             tg = eg.threshold_game(games[g], int(p[g, k]), d)
@@ -357,11 +362,14 @@ def run_batched(args):
         k = int(rng.integers(0, K))
         tg = eg.threshold_game(games[g], int(p[g, k]), d)
         with eg.ResidentGame(tg) as r:
-            _, pst = r.solve()
+            status, pst = r.solve(raise_on_error=False, timeout_ms=1e3 * args.batch_timeout_s)
+            if status != 0:
+                progress(f"plain pair: game {g} n={tg.num_nodes} stopped by the time limit")
+                continue
             plain_ms += pst.solve_ms
             plain_pairs += 1
             progress(f"plain pair {plain_pairs}: game {g} n={tg.num_nodes} {pst.solve_ms:.1f} ms")
-    plain = plain_pairs / K / (plain_ms / 1e3)
+    plain = plain_pairs / K / (plain_ms / 1e3) if plain_pairs else None
     last = stats[-1]
     b.free()
     line = {"metric": f"batched games/s (cfg4 stream, first {G} of 4096 uneven games x 8 mean-payoff thresholds, "
@@ -369,13 +377,14 @@ def run_batched(args):
             "value": value, "unit": "games/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int64",
             "data": "synthetic",
+            "games_solved": done, "batch_timeout_s": args.batch_timeout_s,
             "config": {"workload": "batched uneven games", "games": G, "thresholds": K, "d": d,
                        "total_nodes": last.total_nodes, "total_edges": last.total_edges, "block": block,
                        "graph_replayed": last.graph_replayed, "setup_s": setup_s},
             "thresholds_per_s": value * K, "gteps": last.edges / (last.solve_ms * 1e6),
             "plain": {"games_per_s": plain, "sample_pairs": plain_pairs,
                       "how": "eg_dgame solve per (game, threshold), device time, seeded sample"},
-            "speedup_vs_plain": value / plain, "clocks": clocks,
+            "speedup_vs_plain": value / plain if plain else None, "clocks": clocks,
             "solve": {"rounds_max": last.rounds_max, "rounds_sum": last.rounds_sum, "lifts": last.lifts,
                       "edges": last.edges, "num_top": last.num_top, "grid": last.grid}}
     print(json.dumps(line), flush=True)
