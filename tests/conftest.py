@@ -29,8 +29,11 @@ def _built():
 
 
 def load_solution(path: Path) -> dict[int, int]:
+    import gzip
+
+    text = gzip.open(path, "rt").read() if path.suffix == ".gz" else path.read_text()
     out = {}
-    for line in path.read_text().splitlines():
+    for line in text.splitlines():
         k, v = line.split()
         out[int(k)] = int(v)
     return out
@@ -63,3 +66,13 @@ def golden_fig2():
 
     g = eg.read_game(str(GOLDEN / "eg_fig2.txt"))
     return g, load_solution(GOLDEN / "eg_fig2.sol")
+
+
+@pytest.fixture(scope="session")
+def golden_ieee1394():
+    """The reference's 571,378-vertex model-checking game with the solution
+    its own driver prints."""
+    import egsolver_b200 as eg
+
+    g = eg.read_game(str(GOLDEN / "ieee1394_p4.txt.gz"))
+    return g, load_solution(GOLDEN / "ieee1394_p4.sol.gz")

@@ -9,6 +9,9 @@ Reads, from the reference project (fvella/EGSolver):
                                  --cpu`, lines 43-2043 "ext)<TAB>credit")
   script/multi/eg_fig2.txt       5-vertex example game (no expected output
                                  ships with it)
+  dataset/test/modelchecking/IEEE1394nparties=2_datasize=2_headersize=2_
+  acksize=2_property4.mpg.gz     a 571,378-vertex game from model checking
+                                 (no expected output ships with it)
 
 and writes:
   clique_500_cp4.txt.gz   the same game re-serialised by this library's
@@ -18,11 +21,17 @@ and writes:
   eg_fig2.sol             its credits, [0, 3, TOP, 0, TOP] for vertices 0..4:
                           derived by hand and confirmed by running the
                           reference's own driver (oracle/_ref/egsolver --cpu)
+  ieee1394_p4.txt.gz      the model-checking game, re-serialised
+  ieee1394_p4.sol.gz      "ext credit" per vertex as printed by the
+                          reference's own driver (oracle/_ref/egsolver --cpu
+                          --eg, built by `make -C oracle ref`)
 
 The fixtures are committed; the GPU box has no reference tree.
 """
 from __future__ import annotations
 
+import gzip
+import subprocess
 import sys
 from pathlib import Path
 
@@ -55,6 +64,16 @@ def main(ref: Path) -> None:
     (HERE / "eg_fig2.txt").write_text(eg.game_to_text(fig))
     top = 2147483647
     (HERE / "eg_fig2.sol").write_text("".join(f"{k} {v}\n" for k, v in enumerate([0, 3, top, 0, top])))
+    mc = ref / "dataset" / "test" / "modelchecking" / (
+        "IEEE1394nparties=2_datasize=2_headersize=2_acksize=2_property4.mpg.gz")
+    eg.write_game_text(eg.read_game(str(mc)), str(HERE / "ieee1394_p4.txt.gz"))
+    drv = HERE.parents[1] / "oracle" / "_ref" / "egsolver"
+    out = subprocess.run([str(drv), "--cpu", "--eg", "--input", str(mc)], capture_output=True, text=True,
+                         check=True, timeout=3600).stdout
+    sol = parse_solution(out)
+    assert len(sol) == 571378, len(sol)
+    with gzip.open(HERE / "ieee1394_p4.sol.gz", "wt") as f:
+        f.write("".join(f"{k} {v}\n" for k, v in sorted(sol)))
     print("wrote fixtures to", HERE)
 
 

@@ -355,3 +355,11 @@ def test_reference_driver_runs_unchanged_on_the_gpu(shuffling):
             k, v = line.split(")")
             sol[int(k)] = int(v)
     assert sol == load_solution(GOLDEN / "clique_500_cp4.sol")
+
+
+def test_ieee1394_model_checking_game(golden_ieee1394):
+    """A real game from the reference's dataset (571,378 vertices, mostly
+    out-degree 1 and 2) against the solution the reference's driver prints."""
+    game, sol = golden_ieee1394
+    f, _ = eg.solve(game, credit_bits=32)
+    assert by_ext(game, f) == sol

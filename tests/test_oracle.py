@@ -130,3 +130,11 @@ def test_count_inconsistent_detects_a_planted_error():
     i = int(np.flatnonzero(bad < O.TOP64)[0])
     bad[i] += 1
     assert O.count_inconsistent(g, bad) >= 1
+
+
+def test_ieee1394_model_checking_game_matches_the_reference_driver(golden_ieee1394):
+    game, sol = golden_ieee1394
+    assert game.num_nodes == 571378 and game.num_edges == 996970
+    f, st = O.eg_solve(game, bits=32)
+    assert st["finished"] and st["loops"] == 64725026  # the reference driver's own pop count
+    assert by_ext(game, f) == sol
