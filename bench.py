@@ -216,7 +216,9 @@ def cpu_sample_omp(game, seconds: float):
     secs, threads)."""
     from oracle import oracle as O
 
-    threads = os.cpu_count() or 1
+    # the reference indexes a per-thread array sized MAX_THREADS (256 in
+    # oracle/Makefile) by the thread id
+    threads = min(os.cpu_count() or 1, 256)
     S = 4
     _, st = O.ref_cpu_solve(game, "eg0", threads=threads, max_loop_=S)
     S = max(S, int(S * seconds / max(st["seconds"], 1e-3)))
