@@ -249,6 +249,15 @@ extern "C" void eg_dgame_free(eg_dgame *g)
 
 static eg_status dgame_alloc(const eg_game *game, const eg_opts *opts, eg_dgame **out)
 {
+    {
+        /* the padded row offsets (up to one pad pair per vertex) and the
+         * padded predecessor offsets (up to three pads per vertex) are int */
+        const long long npc = align32(game->num_nodes) + 32LL * (EG_MAX_CLASSES + 1);
+        if (game->num_edges + 3 * npc + 64 > (long long)INT32_MAX)
+            return eg_set_error(EG_ERR_INVALID,
+                                "game too large: %lld edges plus padding for %d vertices exceed 32-bit offsets",
+                                (long long)game->num_edges, game->num_nodes);
+    }
     const int dev = opts ? opts->device : 0;
     int count = 0;
     if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0) {

@@ -2,27 +2,32 @@
  * eg_noalloc.cu -- a CSR -> CSC transpose on device buffers that allocates
  * nothing.
  *
- * Some callers of this library cannot allocate device memory at the moment
- * they need a transpose: code running while a CUDA stream is being captured
- * into a graph (cudaMalloc is not allowed there), runtimes that hand every
- * byte of device memory to their own pool up front, and hosts that forbid
- * allocation after start-up.  They pass their own input and output buffers;
- * the temporaries of the counting sort live in one file-scope __device__
- * array of fixed size instead of in cudaMalloc'd scratch.
+ * Who needs it: a caller that is not allowed to allocate device memory at
+ * the moment it wants a transpose.  Typical cases are an application that
+ * hands all of a GPU's memory to its own pool at start-up (a cudaMalloc
+ * from inside it then fails, or steals memory the pool has promised to
+ * someone else), a serving process whose latency budget has no room for
+ * cudaMalloc / cudaFree (cudaFree waits for the whole device), and a plugin
+ * whose host application forbids allocation after initialisation.  Such a
+ * caller passes its own input and output buffers; the temporaries of the
+ * counting sort live in one file-scope __device__ array of fixed size
+ * instead of in cudaMalloc'd scratch.
  *
  * The array holds room for EG_NOALLOC_MAX_NNZ entries and
  * EG_NOALLOC_MAX_COLS columns (about 25 MB).  Every GPU that loads the
  * library keeps it until the process exits.  All calls share it, so two
  * calls whose work overlaps on the GPU (on different streams, or from
  * different host threads) race on it.  The array keeps the contents of the
- * last call; the column counters and the error word are cleared by every
- * call before use.
+ * last call; each call clears the column counters and the error word and
+ * rewrites every sort entry below its nnz before anything reads them.
  *
  * Host code cannot name the array as a device address: its name on the
  * host is only a stand-in for the symbol.  So, once per device, with that
  * device current, the first call asks the runtime for the array's device
- * address (cudaGetSymbolAddress) and caches it; that first call on a device
- * should therefore come before any stream capture.
+ * address (cudaGetSymbolAddress, return code checked) and caches it; that
+ * first call on a device should therefore come before any stream capture.
+ * Each call ends by reading the error word back and synchronising the
+ * stream.
  */
 #include "eg_prep.cuh"
 
@@ -46,6 +51,19 @@ constexpr long long kOffSort = kOffError + 32;
 pthread_mutex_t g_lock = PTHREAD_MUTEX_INITIALIZER;
 constexpr int kMaxDevices = 64;
 int *g_addr[kMaxDevices];
+
+/* Every sort entry below nnz gets a defined key, edge index and row before
+ * the expansion runs, so that entries a malformed row_ptr leaves unvisited
+ * still hold in-range values (the sort and the gather then read only
+ * indexes below nnz), never the leftovers of an earlier, larger call. */
+__global__ void k_noalloc_init(long long nnz, int *key, int *val, int *rows)
+{
+    for (long long j = (long long)blockIdx.x * blockDim.x + threadIdx.x; j < nnz; j += (long long)gridDim.x * blockDim.x) {
+        key[j] = 0;
+        val[j] = (int)j;
+        rows[j] = 0;
+    }
+}
 
 /* Rows with offsets outside [0, nnz] or not monotone, and columns outside
  * [0, num_cols), are skipped and flagged in the error word instead of being
@@ -152,6 +170,7 @@ extern "C" eg_status eg_csr2csc_device_noalloc(int32_t num_rows, int32_t num_col
     cudaError_t e = cudaMemsetAsync(counts, 0, sizeof(int) * ((size_t)num_cols + 1), cs);
     if (e == cudaSuccess) e = cudaMemsetAsync(err, 0, sizeof(int), cs);
     if (e != cudaSuccess) return eg_set_error(EG_ERR_CUDA, "cudaMemsetAsync failed: %s", cudaGetErrorString(e));
+    k_noalloc_init<<<grid_of(nnz, 256), 256, 0, cs>>>(nnz, k0, v0, rows);
     k_noalloc_expand<<<grid_of((long long)num_rows * 32, 256), 256, 0, cs>>>(num_rows, num_cols, nnz, (const long long *)row_ptr, col_idx,
                                                                               k0, v0, rows, counts, err);
     excl_scan(counts, (long long)num_cols + 1, sort, cs);

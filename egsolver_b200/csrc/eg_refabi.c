@@ -4,12 +4,12 @@
  * runs unchanged against the B200 solver.
  *
  * Exported symbols, with the reference declarations they replace:
- *   int  alloca_memoria_host(void)      reference src/dev_solver.h:9,  src/dev_solver.cu:178-213
- *   int  alloca_memoria_device(void)    reference src/dev_solver.h:10, src/dev_solver.cu:219-265
- *   int  copia_dati_su_device(void)     reference src/dev_solver.h:15, src/dev_solver.cu:168-175
- *   void gpu_solver(void)               reference src/dev_solver.h:20, src/dev_solver.cu:107-165
- *   int  dealloca_memoria_host(void)    reference src/dev_solver.h:12, src/dev_solver.cu:267-286
- *   int  dealloca_memoria_device(void)  reference src/dev_solver.h:13, src/dev_solver.cu:288-292
+ *   int  alloca_memoria_host(void)      reference src/dev_solver.h:9,  src/dev_solver.cu:152-191
+ *   int  alloca_memoria_device(void)    reference src/dev_solver.h:10, src/dev_solver.cu:193-239
+ *   int  copia_dati_su_device(void)     reference src/dev_solver.h:15, src/dev_solver.cu:142-150
+ *   void gpu_solver(void)               reference src/dev_solver.h:20, src/dev_solver.cu:81-139
+ *   int  dealloca_memoria_host(void)    reference src/dev_solver.h:12, src/dev_solver.cu:241-260
+ *   int  dealloca_memoria_device(void)  reference src/dev_solver.h:13, src/dev_solver.cu:262-266
  *   void checkDevice(int*, config*)     reference src/utils.h:20,      src/utils.cu:51-75
  *   void checkCUDAError(const char*)    reference src/utils.cu:38-47
  *
@@ -18,7 +18,7 @@
  * the owner-sorted CSR in host_csr*, counter_nodi0, the configuration and
  * statistics structs, and the result in host_ResNodeValues1.  The host
  * buffer layout is the reference's (one pinned block; src/dev_solver.cu:
- * 178-190).  On the device the game becomes one resident eg_dgame.
+ * 152-178).  On the device the game becomes one resident eg_dgame.
  *
  * Like the reference module this file ends the process on errors: the
  * driver that calls it expects that.  The library's own API (eg_*) never

@@ -304,18 +304,21 @@ void eg_batch_free(eg_batch *b);
 /* ------------------------------------------------------------------ */
 
 /* No counterpart in the reference.  The same transpose as eg_csr2csc_i32,
- * for callers that cannot allocate device memory when they need it (code
- * running during CUDA stream capture, runtimes that own all device memory
- * in their own pool, hosts that forbid allocation after start-up).  All
- * pointers are device pointers owned by the caller; stream is a
- * cudaStream_t (NULL: the legacy default stream).  Temporaries live in one
- * static device array sized for EG_NOALLOC_MAX_NNZ entries and
- * EG_NOALLOC_MAX_COLS columns (about 25 MB, held by every GPU that loads the
- * library until exit); larger inputs are rejected with EG_ERR_INVALID.  The
- * call never allocates, and returns after the transpose has finished on the
- * stream.  The first call on each device looks the static array up
- * (cudaGetSymbolAddress), so make it before any stream capture.  Calls that
- * overlap on the GPU share the array and race; serialise them. */
+ * for callers that must not allocate device memory when they need it: an
+ * application that gives all of a GPU's memory to its own pool at start-up,
+ * a serving process that cannot afford cudaMalloc / cudaFree (cudaFree
+ * waits for the whole device) on its request path, or a plugin whose host
+ * forbids allocation after initialisation.  All pointers are device
+ * pointers owned by the caller; stream is a cudaStream_t (NULL: the legacy
+ * default stream).  Temporaries live in one static device array sized for
+ * EG_NOALLOC_MAX_NNZ entries and EG_NOALLOC_MAX_COLS columns (about 25 MB,
+ * held by every GPU that loads the library until the process exits);
+ * larger inputs are rejected with EG_ERR_INVALID.  The call allocates
+ * nothing, reads the error word back and synchronises the stream before it
+ * returns.  The first call on each device looks the static array up
+ * (cudaGetSymbolAddress), so make that first call before any stream
+ * capture.  Every call shares the array: calls that overlap on the GPU
+ * race, so serialise them. */
 #define EG_NOALLOC_MAX_NNZ (1LL << 20)
 #define EG_NOALLOC_MAX_COLS (1LL << 20)
 eg_status eg_csr2csc_device_noalloc(int32_t num_rows, int32_t num_cols, int64_t nnz,

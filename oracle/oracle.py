@@ -26,7 +26,9 @@ HERE = Path(__file__).resolve().parent
 LIB = HERE / "liboracle.so"
 REF_LIB = HERE / "_ref" / "libegref.so"
 REF_BIN = HERE / "_ref" / "egsolver"
-REF_TREE = Path(os.environ.get("EG_REFERENCE_TREE", "/root/reference"))
+# the reference checkout: $EG_REFERENCE_TREE, else a directory named "reference"
+# beside this repository
+REF_TREE = Path(os.environ.get("EG_REFERENCE_TREE", str(HERE.parent.parent / "reference")))
 
 TOP32 = 2147483647
 TOP64 = 9223372036854775807

@@ -31,6 +31,7 @@ The fixtures are committed; the GPU box has no reference tree.
 from __future__ import annotations
 
 import gzip
+import os
 import subprocess
 import sys
 from pathlib import Path
@@ -78,4 +79,6 @@ def main(ref: Path) -> None:
 
 
 if __name__ == "__main__":
-    main(Path(sys.argv[1]) if len(sys.argv) > 1 else Path("/root/reference"))
+    # the reference checkout: argv[1], $EG_REFERENCE_TREE, else "reference" beside this repository
+    default = os.environ.get("EG_REFERENCE_TREE", str(HERE.parents[2] / "reference"))
+    main(Path(sys.argv[1]) if len(sys.argv) > 1 else Path(default))
