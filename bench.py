@@ -97,13 +97,39 @@ def load_workload(name: str, n: int):
     return fn(n) if n else fn()
 
 
-def workload_config(name: str, game) -> dict:
+def workload_config(name: str, game, world: int) -> dict:
     deg = np.diff(game.row_ptr)
-    return {"workload": {"cfg1": "random 4-regular game", "cfg2": "single large sparse game",
-                         "cfg3": "dense clique game"}[name],
-            "n": game.num_nodes, "m": game.num_edges, "max_out_degree": int(deg.max()),
-            "mean_out_degree": round(float(deg.mean()), 3), "weights": f"+-{game.max_abs_weight}",
-            "credits": "int64", "seed": "0xE6+cfg", "l2": "flushed (256 MB write) before every step"}
+    cfg = {"workload": {"cfg1": "random 4-regular game", "cfg2": "single large sparse game",
+                        "cfg3": "dense clique game"}[name],
+           "n": game.num_nodes, "m": game.num_edges, "max_out_degree": int(deg.max()),
+           "mean_out_degree": round(float(deg.mean()), 3), "weights": f"+-{game.max_abs_weight}",
+           "credits": "int64", "seed": "0xE6+cfg", "l2": "flushed (256 MB write) before every step",
+           "parallelism": f"replicas x{world}" if world > 1 else "single GPU"}
+    if name == "cfg2" and game.num_nodes == 1 << 20:
+        cfg["degree_law"] = ("floor of a continuous x^-2 law on [1, 4097), clipped to [1, 4096]: mean 7.9 and "
+                             "m = 8,309,547, against the configuration's approximate 8.4M")
+    return cfg
+
+
+def cpu_model() -> str:
+    try:
+        for line in Path("/proc/cpuinfo").read_text().splitlines():
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
+def full_size_pin(name: str, game):
+    """The committed Jacobi pin of this workload (sweeps of the full solve), if any."""
+    p = ROOT / "tests" / "golden" / f"{name}_full_size.json"
+    if not p.exists():
+        return None
+    d = json.loads(p.read_text())
+    if d.get("n") != game.num_nodes or d.get("m") != game.num_edges or "sweeps" not in d:
+        return None
+    return d
 
 
 class ClockSampler:
@@ -212,8 +238,11 @@ def cpu_sample(game, seconds: float, kind_pref: str = "reference"):
 def cpu_sample_omp(game, seconds: float):
     """Times the reference's own OpenMP EG0 (Jacobi sweeps, cpu_solver.c
     EG0_cpu_solver, compiled unmodified) on all host cores for its first S
-    sweeps of `game`; every sweep scans all m edges.  Returns (gteps, S,
-    secs, threads)."""
+    sweeps of `game`; every sweep scans all m edges.  Its inner index is
+    shared between threads (reference src/cpu_solver.c:111,146-157), so its
+    credits after the S sweeps are compared with the race-free restatement's
+    after the same S sweeps (Jacobi sweeps are deterministic): a mismatch
+    marks the timing invalid.  Returns (gteps, S, secs, threads, valid)."""
     from oracle import oracle as O
 
     # the reference indexes a per-thread array sized MAX_THREADS (256 in
@@ -222,17 +251,35 @@ def cpu_sample_omp(game, seconds: float):
     S = 4
     _, st = O.ref_cpu_solve(game, "eg0", threads=threads, max_loop_=S)
     S = max(S, int(S * seconds / max(st["seconds"], 1e-3)))
-    _, st = O.ref_cpu_solve(game, "eg0", threads=threads, max_loop_=S)
-    return game.num_edges * S / st["seconds"] / 1e9, S, st["seconds"], threads
+    f_ref, st = O.ref_cpu_solve(game, "eg0", threads=threads, max_loop_=S)
+    f_fix, _ = O.eg0_solve(game, threads=threads, max_loop_=S)
+    valid = bool(np.array_equal(f_ref, f_fix))
+    return game.num_edges * S / st["seconds"] / 1e9, S, st["seconds"], threads, valid
+
+
+def time_to_solution(name: str, game, omp_sweeps: int, omp_secs: float, threads: int, valid: bool):
+    """Projected full-solve time of the reference's OpenMP EG0 on this box:
+    the committed pin's sweep count x the measured time per sweep."""
+    pin = full_size_pin(name, game)
+    if pin is None or omp_sweeps <= 0:
+        return None
+    per_sweep = omp_secs / omp_sweeps
+    return {"reference_eg0_projected_s": pin["sweeps"] * per_sweep, "sweeps": pin["sweeps"],
+            "per_sweep_ms": 1e3 * per_sweep, "threads": threads, "eg0_output_valid": valid,
+            "how": "sweeps of the full Jacobi solve (committed pin tests/golden/" + name + "_full_size.json) x "
+                   "the reference EG0's measured time per sweep on this box's cores"}
 
 
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
     if rank != 0:
         return
-    game = load_workload(args.workload, args.n)
     from oracle import oracle as O
 
+    # the game comes from the oracle's restated generator: this arm loads no
+    # part of the solver library
+    game = O.workload(args.workload, args.n)
     use_ref = O.ref_available()
     # every step is a bounded sample of the workload, sized so that all
     # warm-up and timed steps take about a minute together
@@ -258,17 +305,23 @@ def run_reference(args):
         for _ in range(args.warmup):
             step()
         times = [step() for _ in range(args.steps)]
+        tts = None
+        if use_ref and full_size_pin(args.workload, game) is not None:
+            _, S, osecs, th, valid = cpu_sample_omp(game, 10.0)
+            tts = time_to_solution(args.workload, game, S, osecs, th, valid)
     total = sum(times)
     value = edges * args.steps / total / 1e9
     kind = "reference" if use_ref else "port"
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * total / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int32", "data": "synthetic",
-            "config": workload_config(args.workload, game),
-            "cpu_baseline": {"value": value, "unit": UNIT, "cores": 1, "kind": kind,
+            "config": workload_config(args.workload, game, world),
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": 1, "kind": kind, "cpu_model": cpu_model(),
+                             "omp_num_threads": os.environ.get("OMP_NUM_THREADS", "unset"),
                              "sample": f"first {P} worklist pops of EG_cpu_solver (reference --eg {P}) on the "
                                        f"same game, {edges} edges relaxed per step"},
-            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "time_to_solution": tts}
     print(json.dumps(line), flush=True)
 
 
@@ -484,8 +537,7 @@ def main():
     torch.cuda.set_device(local)
     game = load_workload(args.workload, args.n)
     credit_bits = 64
-    cfg = workload_config(args.workload, game)
-    cfg["parallelism"] = f"replicas x{world}" if world > 1 else "single GPU"
+    cfg = workload_config(args.workload, game, world)
 
     res = eg.ResidentGame(game, device=local)
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.int32, device=f"cuda:{local}")
@@ -599,20 +651,28 @@ def main():
                 "traffic": traffic, "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)",
                 "kernel": kernel, "algorithmic_bytes_per_launch": per_launch, **extra}
 
-    cpu = cpu_omp = None
+    cpu = cpu_omp = tts = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         with stdout_to_stderr():
             g, ed, secs, P, kind = cpu_sample(game, args.cpu_sample_s)
-        cpu = {"value": g, "unit": UNIT, "cores": 1, "kind": kind,
+        cpu = {"value": g, "unit": UNIT, "cores": 1, "kind": kind, "cpu_model": cpu_model(),
+               "omp_num_threads": os.environ.get("OMP_NUM_THREADS", "unset"),
                "sample": f"first {P} worklist pops of EG_cpu_solver (reference --eg {P}) on the same game: "
                          f"{ed} edges in {secs:.2f} s"}
         if kind == "reference":
             with stdout_to_stderr():
-                og, S, osecs, th = cpu_sample_omp(game, args.cpu_sample_s / 2)
-            cpu_omp = {"value": og, "unit": UNIT, "cores": th, "kind": "reference",
-                       "sample": f"first {S} sweeps of the reference's OpenMP EG0_cpu_solver (--eg0, {th} threads; "
-                                 f"its shared inner index races, so only the timing is used): {S} x m edges in "
-                                 f"{osecs:.2f} s"}
+                og, S, osecs, th, valid = cpu_sample_omp(game, args.cpu_sample_s / 2)
+            cpu_omp = {"value": og if valid else None, "unit": UNIT, "cores": th, "kind": "reference",
+                       "valid": valid, "measured_gteps": og,
+                       "sample": f"first {S} sweeps of the reference's OpenMP EG0_cpu_solver (--eg0, {th} threads): "
+                                 f"{S} x m edges in {osecs:.2f} s; its credits after these sweeps "
+                                 f"{'equal' if valid else 'DIFFER from'} the race-free restatement's"}
+            tts = time_to_solution(args.workload, game, S, osecs, th, valid)
+            if tts is not None:
+                tts["gpu_solve_s"] = dev_ms_max / args.steps / 1e3
+                if e2e is not None:
+                    tts["gpu_e2e_s"] = e2e["ms_per_step"] / 1e3
+                    tts["speedup_e2e_vs_reference_eg0"] = tts["reference_eg0_projected_s"] / tts["gpu_e2e_s"]
 
     if rank == 0:
         if capped:
@@ -622,6 +682,7 @@ def main():
                 "scaling": "weak", "vs_baseline": None, "dtype": f"int{last.credit_bits}", "data": "synthetic",
                 "config": cfg,
                 "roofline": roofline, "cpu_baseline": cpu, "cpu_baseline_omp": cpu_omp, "e2e": e2e,
+                "time_to_solution": tts,
                 "gpu_launches": int(launches),
                 "clocks": clocks,
                 "solve": {"rounds": last.rounds, "lifts": last.lifts, "edges": last.edges, "changes": last.changes,

@@ -33,7 +33,7 @@ NVCC_FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "--expt-r
 CC_FLAGS = ["-O3", "-fPIC", "-std=gnu11", "-Wall", "-Wno-unused-function", "-I", str(INCLUDE), "-I", str(CSRC),
             "-I", str(CUDA_HOME / "include")]
 
-C_SOURCES = ["eg_host.c", "eg_reader.c"]
+C_SOURCES = ["eg_host.c", "eg_reader.c", "eg_fixtures.c"]
 CU_SOURCES = ["eg_prep.cu", "eg_lift.cu", "eg_dense.cu", "eg_api.cu", "eg_batch.cu", "eg_serve.cu", "eg_noalloc.cu"]
 REFABI_SOURCES = ["eg_refabi.c"]
 

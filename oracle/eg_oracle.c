@@ -14,6 +14,9 @@
  *   oracle_eg0_omp_i32   <- src/cpu_solver.c:109-185 with its two thread-safety
  *                           defects fixed (private inner index, per-thread flags
  *                           sized by the thread count)
+ *   oracle_generate      the benchmark's seeded game generator (not part of the
+ *                        reference), so that reference-side timings build their
+ *                        inputs without the solver library
  *
  * Parity pins: the int32 worklist solver is checked against the reference's
  * own cpu_solver.c compiled under oracle/_ref (same pop count and credits),
@@ -26,6 +29,7 @@
  * offsets are the same numbers.
  */
 #include <limits.h>
+#include <math.h>
 #include <stdint.h>
 #include <stdlib.h>
 #include <string.h>
@@ -290,3 +294,134 @@ int64_t oracle_count_inconsistent_i64(int32_t n, int32_t n0, const int64_t *ptr,
     }
     return bad;
 }
+
+/* ------------------------------------------------------------------ */
+/* Seeded benchmark games, restated for the checker side                */
+/* ------------------------------------------------------------------ */
+
+/* The benchmark's seeded game generator, restated here so that the
+ * reference arm of the benchmark and the CPU baselines build their inputs
+ * without loading the solver library.  Same definition as the library's
+ * eg_generate: splitmix64 (Steele, Lea, Flood 2014) drives, in order, one
+ * owner bit per vertex (the top bit), the out-degrees (kind 1: deg; kind 2:
+ * floor of the inverse-CDF sample 1 / (1 - u (1 - 1/(deg+1))) of a
+ * continuous x^-2 law on [1, deg+1), clipped to [1, deg]; kind 3: n - 1;
+ * kind 4: uniform in [param, deg]; kind 5: 1 + floor(log1p(-u) /
+ * log1p(-1/param)) capped at deg), then per vertex its distinct successors
+ * without self-loops (rejection sampling; kind 3 takes all others in order)
+ * followed by its weights uniform in [-wmax, wmax].  Uniform integers are
+ * the multiply-shift map of the top 32 bits.  The result is renumbered
+ * owner-sorted (player 0 first, each class in increasing index, edge order
+ * kept), the layout the reference's postparsing builds.
+ *
+ * Outputs are malloc'd (free with oracle_free); returns 0, -1 on bad
+ * arguments, -2 on allocation failure. */
+typedef struct { uint64_t s; } orng;
+static inline uint64_t orng_next(orng *r)
+{
+    uint64_t z = (r->s += 0x9e3779b97f4a7c15ULL);
+    z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ULL;
+    z = (z ^ (z >> 27)) * 0x94d049bb133111ebULL;
+    return z ^ (z >> 31);
+}
+static inline uint32_t orng_below(orng *r, uint32_t bound)
+{
+    return (uint32_t)(((orng_next(r) >> 32) * (uint64_t)bound) >> 32);
+}
+static inline double orng_unit(orng *r) { return (double)(orng_next(r) >> 11) * (1.0 / 9007199254740992.0); }
+
+int oracle_generate(int32_t kind, int32_t n, int32_t deg, int32_t wmax, int32_t param, uint64_t seed,
+                    int64_t **ptr_out, int32_t **succ_out, int32_t **w_out, int64_t *m_out, int32_t *n0_out)
+{
+    if (n < 2 || wmax < 0 || kind < 1 || kind > 5) return -1;
+    if (kind != 3 && (deg < 1 || deg > n - 1)) return -1;
+    if (kind == 4 && (param < 1 || param > deg)) return -1;
+    if (kind == 5 && param < 1) return -1;
+    orng r = {seed};
+    uint8_t *own = malloc((size_t)n);
+    int64_t *deg_of = malloc(sizeof(int64_t) * (size_t)n);
+    int32_t *seen = calloc((size_t)n, sizeof(int32_t));
+    if (!own || !deg_of || !seen) {
+        free(own); free(deg_of); free(seen);
+        return -2;
+    }
+    for (int32_t v = 0; v < n; v++) own[v] = (uint8_t)(orng_next(&r) >> 63);
+    int64_t m = 0;
+    for (int32_t v = 0; v < n; v++) {
+        int64_t d;
+        if (kind == 1) {
+            d = deg;
+        } else if (kind == 2) {
+            const double u = orng_unit(&r);
+            d = (int64_t)floor(1.0 / (1.0 - u * (1.0 - 1.0 / ((double)deg + 1.0))));
+            d = d < 1 ? 1 : (d > deg ? deg : d);
+        } else if (kind == 3) {
+            d = n - 1;
+        } else if (kind == 4) {
+            d = param + (int64_t)orng_below(&r, (uint32_t)(deg - param + 1));
+        } else {
+            const double q = 1.0 / (double)param;
+            d = 1;
+            if (q < 1.0) d = 1 + (int64_t)floor(log1p(-orng_unit(&r)) / log1p(-q));
+            if (d > deg) d = deg;
+        }
+        deg_of[v] = d;
+        m += d;
+    }
+    int32_t *s0 = malloc(sizeof(int32_t) * (size_t)(m > 0 ? m : 1));
+    int32_t *w0 = malloc(sizeof(int32_t) * (size_t)(m > 0 ? m : 1));
+    int64_t *p0 = malloc(sizeof(int64_t) * ((size_t)n + 1));
+    int64_t *ptr = malloc(sizeof(int64_t) * ((size_t)n + 1));
+    int32_t *succ = malloc(sizeof(int32_t) * (size_t)(m > 0 ? m : 1));
+    int32_t *w = malloc(sizeof(int32_t) * (size_t)(m > 0 ? m : 1));
+    int32_t *nid = malloc(sizeof(int32_t) * (size_t)n);
+    int32_t *oid = malloc(sizeof(int32_t) * (size_t)n);
+    if (!s0 || !w0 || !p0 || !ptr || !succ || !w || !nid || !oid) {
+        free(own); free(deg_of); free(seen); free(s0); free(w0); free(p0); free(ptr); free(succ); free(w);
+        free(nid); free(oid);
+        return -2;
+    }
+    p0[0] = 0;
+    for (int32_t v = 0; v < n; v++) p0[v + 1] = p0[v] + deg_of[v];
+    for (int32_t v = 0; v < n; v++) {
+        const int64_t b = p0[v], d = deg_of[v];
+        if (kind == 3) {
+            int64_t k = 0;
+            for (int32_t x = 0; x < n; x++)
+                if (x != v) s0[b + k++] = x;
+        } else {
+            seen[v] = v + 1;
+            for (int64_t k = 0; k < d;) {
+                const int32_t x = (int32_t)orng_below(&r, (uint32_t)n);
+                if (seen[x] == v + 1) continue;
+                seen[x] = v + 1;
+                s0[b + k++] = x;
+            }
+        }
+        for (int64_t k = 0; k < d; k++) w0[b + k] = -wmax + (int32_t)orng_below(&r, (uint32_t)(2 * wmax + 1));
+    }
+    int32_t n0 = 0;
+    for (int32_t v = 0; v < n; v++) n0 += own[v] == 0;
+    int32_t c0 = 0, c1 = n0;
+    for (int32_t v = 0; v < n; v++) nid[v] = own[v] == 0 ? c0++ : c1++;
+    for (int32_t v = 0; v < n; v++) oid[nid[v]] = v;
+    int64_t e = 0;
+    for (int32_t u = 0; u < n; u++) {
+        const int32_t v = oid[u];
+        ptr[u] = e;
+        for (int64_t j = p0[v]; j < p0[v + 1]; j++, e++) {
+            succ[e] = nid[s0[j]];
+            w[e] = w0[j];
+        }
+    }
+    ptr[n] = e;
+    free(own); free(deg_of); free(seen); free(s0); free(w0); free(p0); free(nid); free(oid);
+    *ptr_out = ptr;
+    *succ_out = succ;
+    *w_out = w;
+    *m_out = m;
+    *n0_out = n0;
+    return 0;
+}
+
+void oracle_free(void *p) { free(p); }

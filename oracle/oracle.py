@@ -72,6 +72,12 @@ def lib() -> C.CDLL:
         L.oracle_csr2csc.restype = None
         L.oracle_count_inconsistent_i64.argtypes = [I32, I32, P, P, P, I64, P]
         L.oracle_count_inconsistent_i64.restype = I64
+        L.oracle_generate.argtypes = [I32, I32, I32, I32, I32, C.c_uint64, C.POINTER(C.POINTER(C.c_int64)),
+                                      C.POINTER(C.POINTER(C.c_int32)), C.POINTER(C.POINTER(C.c_int32)),
+                                      C.POINTER(C.c_int64), C.POINTER(C.c_int32)]
+        L.oracle_generate.restype = C.c_int
+        L.oracle_free.argtypes = [P]
+        L.oracle_free.restype = None
         _lib = L
     return _lib
 
@@ -214,3 +220,59 @@ def ref_host_csr2csc(nrow: int, ncol: int, row_ptr, col, val):
     L.host_csr2csc(nrow, ncol, nnz, val.ctypes.data, col.ctypes.data, row_ptr.ctypes.data, cv.ctypes.data,
                    cr.ctypes.data, cp.ctypes.data)
     return cp.astype(np.int64), cr[:nnz], cv[:nnz]
+
+
+class OracleGame:
+    """A generated game in the same CSR form as the solver's Game (host
+    arrays, owner-sorted: vertices [0, num_nodes0) belong to player 0)."""
+
+    def __init__(self, row_ptr, succ, weight, num_nodes0):
+        self.row_ptr, self.succ, self.weight, self.num_nodes0 = row_ptr, succ, weight, int(num_nodes0)
+        self.owner = None
+        self.max_abs_weight = int(np.abs(weight.astype(np.int64)).max()) if weight.size else 0
+
+    @property
+    def num_nodes(self) -> int:
+        return int(self.row_ptr.shape[0] - 1)
+
+    @property
+    def num_edges(self) -> int:
+        return int(self.succ.shape[0])
+
+
+def generate(kind: int, n: int, deg: int, wmax: int, seed: int, param: int = 0) -> OracleGame:
+    """The benchmark's seeded generator, restated in eg_oracle.c (same games as
+    the solver library's eg_generate, without loading that library)."""
+    L = lib()
+    pp, sp, wp = C.POINTER(C.c_int64)(), C.POINTER(C.c_int32)(), C.POINTER(C.c_int32)()
+    m, n0 = C.c_int64(), C.c_int32()
+    rc = L.oracle_generate(kind, n, deg, wmax, param, seed & (2**64 - 1), C.byref(pp), C.byref(sp), C.byref(wp),
+                           C.byref(m), C.byref(n0))
+    if rc != 0:
+        raise ValueError(f"oracle_generate failed ({rc})")
+    try:
+        ptr = np.ctypeslib.as_array(pp, shape=(n + 1,)).copy()
+        succ = np.ctypeslib.as_array(sp, shape=(max(m.value, 1),))[: m.value].copy()
+        w = np.ctypeslib.as_array(wp, shape=(max(m.value, 1),))[: m.value].copy()
+    finally:
+        for q in (pp, sp, wp):
+            L.oracle_free(C.cast(q, C.c_void_p))
+    return OracleGame(ptr, succ, w, n0.value)
+
+
+SEED = 0xE6  # seed base of the benchmark workloads: SEED + configuration number
+
+
+def workload(name: str, n: int = 0) -> OracleGame:
+    """The single-game benchmark workloads (configurations 1-3) built by the
+    restated generator, with the same kinds, bounds and seeds as the solver
+    package's workloads module."""
+    if name == "cfg1":
+        return generate(1, n or 1000, 4, 10, SEED + 1)
+    if name == "cfg2":
+        n = n or (1 << 20)
+        return generate(2, n, min(4096, n - 1), 1000, SEED + 2)
+    if name == "cfg3":
+        n = n or 2000
+        return generate(3, n, n - 1, 500, SEED + 3)
+    raise ValueError(f"unknown workload {name}")

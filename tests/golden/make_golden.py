@@ -18,6 +18,9 @@ and writes:
                           writer (same vertices, owners, edge order, weights)
   clique_500_cp4.sol      "ext credit" per vertex, from sol.txt
   eg_fig2.txt             the example game, re-serialised
+  ref_eg_fig2*.txt        the example game and the reference's shipped
+                          copies of it (script/multi: 2 copies, 4 copies, 2
+                          copies of 2 copies), byte for byte
   eg_fig2.sol             its credits, [0, 3, TOP, 0, TOP] for vertices 0..4:
                           derived by hand and confirmed by running the
                           reference's own driver (oracle/_ref/egsolver --cpu)
@@ -63,6 +66,10 @@ def main(ref: Path) -> None:
     (HERE / "clique_500_cp4.sol").write_text("".join(f"{k} {v}\n" for k, v in sorted(sol)))
     fig = eg.read_game(str(ref / "script" / "multi" / "eg_fig2.txt"))
     (HERE / "eg_fig2.txt").write_text(eg.game_to_text(fig))
+    # the example game and the reference's own multi outputs of it, verbatim
+    # (byte-level fixtures of the copies generator)
+    for name in ("eg_fig2", "eg_fig2_duecopie", "eg_fig2_quattrocopie", "eg_fig2_duecopie_di_duecopie"):
+        (HERE / f"ref_{name}.txt").write_bytes((ref / "script" / "multi" / f"{name}.txt").read_bytes())
     top = 2147483647
     (HERE / "eg_fig2.sol").write_text("".join(f"{k} {v}\n" for k, v in enumerate([0, 3, top, 0, top])))
     mc = ref / "dataset" / "test" / "modelchecking" / (

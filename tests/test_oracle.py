@@ -138,3 +138,28 @@ def test_ieee1394_model_checking_game_matches_the_reference_driver(golden_ieee13
     f, st = O.eg_solve(game, bits=32)
     assert st["finished"] and st["loops"] == 64725026  # the reference driver's own pop count
     assert by_ext(game, f) == sol
+
+
+@pytest.mark.parametrize("args", [(1, 500, 4, 10, 7, 0), (2, 4096, 4095, 1000, 0xE6 + 2, 0), (3, 60, 59, 500, 9, 0),
+                                  (4, 700, 16, 100, 11, 2), (5, 900, 256, 40, 12, 6)])
+def test_restated_generator_equals_the_library_generator(args):
+    """The reference arm builds its games with the oracle's restated generator;
+    it must produce the library's games exactly."""
+    kind, n, deg, wmax, seed, param = args
+    a = eg.generate(kind, n, deg, wmax, seed, param=param)
+    b = O.generate(kind, n, deg, wmax, seed, param=param)
+    assert a.num_nodes0 == b.num_nodes0
+    np.testing.assert_array_equal(a.row_ptr, b.row_ptr)
+    np.testing.assert_array_equal(a.succ, b.succ)
+    np.testing.assert_array_equal(a.weight, b.weight)
+
+
+def test_oracle_workloads_equal_the_package_workloads():
+    from egsolver_b200 import workloads
+
+    for name, n in (("cfg1", 0), ("cfg2", 1 << 12), ("cfg3", 0)):
+        a = getattr(workloads, name)(n) if n else getattr(workloads, name)()
+        b = O.workload(name, n)
+        np.testing.assert_array_equal(a.row_ptr, b.row_ptr)
+        np.testing.assert_array_equal(a.succ, b.succ)
+        np.testing.assert_array_equal(a.weight, b.weight)
