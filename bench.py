@@ -190,14 +190,14 @@ def measured_peak():
 
 
 def dense_round_bytes(game, credit_bytes: int) -> int:
-    """Algorithmic bytes of one dense sweep: per edge pair (two out-edges,
-    odd degrees padded) 16 B of {succ, w} x 2 and 2 B of metadata, 4 B per
-    32-pair chunk; per out-edge the successor's credit S; per vertex its own
-    credit S.  (Credit writes, S per raise, are added from the raise count.)"""
-    deg = np.diff(game.row_ptr)
-    npairs = int(((deg + 1) // 2).sum())
+    """Algorithmic bytes of one dense sweep, by the per-edge and per-vertex
+    figures of the workload's definition: per scanned edge its successor id
+    (4 B), weight (4 B) and the successor's credit (S); per lifted vertex its
+    two row offsets (8 B) and its own credit (S).  A raised credit's write (S)
+    is added from the raise count.  Layout overheads of the kernel (padding
+    pairs, chunk metadata) are not counted."""
     S = credit_bytes
-    return npairs * 18 + (npairs + 31) // 32 * 4 + game.num_edges * S + game.num_nodes * S
+    return game.num_edges * (8 + S) + game.num_nodes * (8 + S)
 
 
 def lift_traffic_bytes(st, credit_bytes: int) -> float:

@@ -22,7 +22,7 @@ from ._ffi import (DIRECTION_DENSE, DIRECTION_SPARSE, DIRECTION_SWITCH, EG_TOP32
                    VARIANT_AUTO, VARIANT_CTA, VARIANT_SMEM, VARIANT_THREAD, VARIANT_WARP)
 
 __all__ = ["Game", "EGError", "Stats", "solve", "ResidentGame", "Batch", "BatchStats", "Server", "threshold_game",
-           "generate", "read_game", "read_game_text",
+           "generate", "read_game", "read_game_text", "read_game_binary", "write_game_binary", "clique_text", "ladder_text", "copies_text",
            "csr2csc", "compute_mg", "default_max_loop", "device_count", "CancelFlag", "EG_TOP32", "EG_TOP64",
            "lib"]
 
@@ -234,6 +234,19 @@ class ResidentGame:
     def device_bytes(self) -> int:
         return int(lib().eg_dgame_device_bytes(self._h))
 
+    TUNED_KNOBS = ("large_min_deg", "task_edges", "small_max_deg", "dense_sweeps", "dense_depth")
+
+    def tune(self, rounds: int = 300, **kw) -> tuple[dict, dict]:
+        """Autotunes the AUTO layout on capped solves (eg_dgame_tune); returns
+        the chosen knobs (keyword arguments of solve) and the report."""
+        base = make_opts(**kw)
+        out = _ffi.EgOpts()
+        rep = _ffi.EgTuneReport()
+        _check(lib().eg_dgame_tune(self._h, C.byref(base), rounds, C.byref(out), C.byref(rep)))
+        knobs = {k: int(getattr(out, k)) for k in self.TUNED_KNOBS}
+        return knobs, {"candidates": rep.candidates, "from_cache": bool(rep.from_cache),
+                       "default_rate": rep.default_rate, "best_rate": rep.best_rate}
+
     def free(self) -> None:
         if self._h:
             lib().eg_dgame_free(self._h)
@@ -286,6 +299,8 @@ class BatchStats:
     grid: int
     games_failed: int
     graph_replayed: int
+    num_units: int = 0
+    smem_bytes: int = 0
 
     @property
     def gteps(self) -> float:
@@ -297,7 +312,7 @@ class Batch:
     (eg_batch_*).  Threshold p of game g turns every weight w into w*d - p."""
 
     def __init__(self, games: list[Game], thresholds: int, scale: int = 1, block: int = 0, device: int = 0,
-                 max_rounds: int = -1, timeout_ms: float = 0.0, use_graph: bool = False):
+                 max_rounds: int = -1, timeout_ms: float = 0.0, use_graph: bool = False, group_max: int = 0):
         self._h = C.c_void_p()
         self._keep = [g.c_struct() for g in games]
         arr = (_ffi.EgGame * len(games))(*self._keep)
@@ -309,6 +324,7 @@ class Batch:
         o.max_rounds = max_rounds
         o.timeout_ms = timeout_ms
         o.use_graph = 1 if use_graph else 0
+        o.group_max = group_max
         _check(lib().eg_batch_create(arr, len(games), C.byref(o), C.byref(self._h)))
         self.sizes = [g.num_nodes for g in games]
         self.K = thresholds
@@ -420,6 +436,15 @@ class Server:
         _check(lib().eg_serve_stats_get(self._h, C.byref(s)))
         return s.as_dict()
 
+    def trace(self) -> list[dict]:
+        """Device-clock spans of the finished micro-batches (eg_serve_trace)."""
+        n = C.c_int32()
+        _check(lib().eg_serve_trace(self._h, None, 0, C.byref(n)))
+        arr = (_ffi.EgServeSpan * max(n.value, 1))()
+        _check(lib().eg_serve_trace(self._h, arr, n.value, C.byref(n)))
+        return [{"batch": a.batch, "queries": a.queries, "units": a.units, "begin_ms": a.begin_ms,
+                 "end_ms": a.end_ms} for a in arr[:n.value]]
+
     def close(self) -> None:
         if self._h:
             _check(lib().eg_serve_destroy(self._h))
@@ -458,6 +483,31 @@ def _own_to_game(og_ptr) -> Game:
     return g
 
 
+def _take_text(fn, *args) -> str:
+    buf, ln = C.c_void_p(), C.c_size_t()
+    _check(fn(*args, C.byref(buf), C.byref(ln)))
+    try:
+        return C.string_at(buf, ln.value).decode()
+    finally:
+        lib().eg_free_text(buf)
+
+
+def clique_text(number: int) -> str:
+    """The reference's mkclique game text (eg_fixture_clique_text)."""
+    return _take_text(lib().eg_fixture_clique_text, number)
+
+
+def ladder_text(number: int) -> str:
+    """The reference's mkladder game text (eg_fixture_ladder_text)."""
+    return _take_text(lib().eg_fixture_ladder_text, number)
+
+
+def copies_text(text: str, copies: int) -> str:
+    """The reference's multi rewrite of a game text (eg_fixture_copies_text)."""
+    raw = text.encode()
+    return _take_text(lib().eg_fixture_copies_text, raw, len(raw), copies)
+
+
 def generate(kind: int, n: int, deg: int, wmax: int, seed: int, param: int = 0) -> Game:
     """Seeded random game (eg_generate); owner-sorted like the reference layout."""
     out = C.POINTER(_ffi.EgOwnedGame)()
@@ -469,11 +519,43 @@ def _read_opts(weight_mode: int, rnd_lo: int, rnd_hi: int, rnd_seed: int) -> _ff
     return _ffi.EgReadOpts(weight_mode, rnd_lo, rnd_hi, rnd_seed)
 
 
-def read_game(path: str, weight_mode: int = 0, rnd_lo: int = -1, rnd_hi: int = 1, rnd_seed: int = 0) -> Game:
-    """Reads a game in the reference text format (gzip or plain)."""
+def read_game(path: str, weight_mode: int = 0, rnd_lo: int = -1, rnd_hi: int = 1, rnd_seed: int = 0,
+              cache: Optional[str] = None) -> Game:
+    """Reads a game in the reference text format (gzip or plain); with cache,
+    through the binary CSR cache file at that path (eg_read_game_file_cached)."""
     out = C.POINTER(_ffi.EgOwnedGame)()
     ro = _read_opts(weight_mode, rnd_lo, rnd_hi, rnd_seed)
-    _check(lib().eg_read_game_file(str(path).encode(), C.byref(ro), C.byref(out)))
+    if cache is None:
+        _check(lib().eg_read_game_file(str(path).encode(), C.byref(ro), C.byref(out)))
+    else:
+        _check(lib().eg_read_game_file_cached(str(path).encode(), C.byref(ro), str(cache).encode(), C.byref(out)))
+    return _own_to_game(out)
+
+
+def write_game_binary(game: Game, path: str, weight_mode: int = 0, rnd_lo: int = -1, rnd_hi: int = 1,
+                      rnd_seed: int = 0) -> None:
+    """Writes the game to the binary CSR file format (eg_write_game_binary);
+    the reader options are recorded with it.  The game must be owner-sorted
+    (no owner array), as the reader returns it."""
+    if game.owner is not None:
+        raise ValueError("the binary format holds owner-sorted games (num_nodes0 split)")
+    ext = game.ext_id if game.ext_id is not None else np.arange(game.num_nodes, dtype=np.int32)
+    ext = np.ascontiguousarray(ext, dtype=np.int32)
+    og = _ffi.EgOwnedGame()
+    og.game = game.c_struct()
+    og.row_ptr, og.succ, og.weight, og.ext_id = _ptr(game.row_ptr), _ptr(game.succ), _ptr(game.weight), _ptr(ext)
+    og.max_abs_weight = game.max_abs_weight
+    ro = _read_opts(weight_mode, rnd_lo, rnd_hi, rnd_seed)
+    _check(lib().eg_write_game_binary(str(path).encode(), C.byref(og), C.byref(ro)))
+
+
+def read_game_binary(path: str, weight_mode: Optional[int] = None, rnd_lo: int = -1, rnd_hi: int = 1,
+                     rnd_seed: int = 0) -> Game:
+    """Reads a binary CSR file; with weight_mode given, only if it was written
+    with those reader options."""
+    out = C.POINTER(_ffi.EgOwnedGame)()
+    ro = None if weight_mode is None else C.byref(_read_opts(weight_mode, rnd_lo, rnd_hi, rnd_seed))
+    _check(lib().eg_read_game_binary(str(path).encode(), ro, C.byref(out)))
     return _own_to_game(out)
 
 

@@ -125,7 +125,8 @@ class EgBatchOpts(C.Structure):
         ("max_rounds", C.c_int64),
         ("timeout_ms", C.c_double),
         ("use_graph", C.c_int32),
-        ("reserved", C.c_int32 * 7),
+        ("group_max", C.c_int32),
+        ("reserved", C.c_int32 * 6),
     ]
 
 
@@ -145,7 +146,9 @@ class EgBatchStats(C.Structure):
         ("grid", C.c_int32),
         ("games_failed", C.c_int32),
         ("graph_replayed", C.c_int32),
-        ("reserved", C.c_int32 * 4),
+        ("num_units", C.c_int32),
+        ("smem_bytes", C.c_int32),
+        ("reserved", C.c_int32 * 2),
     ]
 
     def as_dict(self) -> dict:
@@ -179,6 +182,16 @@ class EgServeStats(C.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_ if k != "reserved"}
 
 
+class EgTuneReport(C.Structure):
+    _fields_ = [("candidates", C.c_int32), ("from_cache", C.c_int32), ("default_rate", C.c_double),
+                ("best_rate", C.c_double), ("reserved", C.c_int32 * 4)]
+
+
+class EgServeSpan(C.Structure):
+    _fields_ = [("batch", C.c_int64), ("queries", C.c_int32), ("units", C.c_int32), ("begin_ms", C.c_double),
+                ("end_ms", C.c_double)]
+
+
 # every symbol the header declares, with (restype, argtypes)
 _P = C.c_void_p
 _I32, _I64 = C.c_int32, C.c_int64
@@ -199,6 +212,7 @@ SIGNATURES = {
     "eg_dgame_credits_i64": (_I32, [_P, _P]),
     "eg_dgame_credits_device": (_I32, [_P, C.POINTER(_P), C.POINTER(_I32)]),
     "eg_dgame_device_bytes": (_I64, [_P]),
+    "eg_dgame_tune": (_I32, [_P, C.POINTER(EgOpts), _I64, C.POINTER(EgOpts), C.POINTER(EgTuneReport)]),
     "eg_dgame_free": (None, [_P]),
     "eg_csr2csc_i32": (_I32, [_I32, _I32, _I64, _P, _P, _P, _P, _P, _P]),
     "eg_cancel_flag_alloc": (_I32, [C.POINTER(_P)]),
@@ -206,6 +220,10 @@ SIGNATURES = {
     "eg_read_game_file": (_I32, [C.c_char_p, C.POINTER(EgReadOpts), C.POINTER(C.POINTER(EgOwnedGame))]),
     "eg_read_game_buffer": (_I32, [C.c_char_p, C.c_size_t, C.POINTER(EgReadOpts), C.POINTER(C.POINTER(EgOwnedGame))]),
     "eg_owned_game_free": (None, [C.POINTER(EgOwnedGame)]),
+    "eg_write_game_binary": (_I32, [C.c_char_p, C.POINTER(EgOwnedGame), C.POINTER(EgReadOpts)]),
+    "eg_read_game_binary": (_I32, [C.c_char_p, C.POINTER(EgReadOpts), C.POINTER(C.POINTER(EgOwnedGame))]),
+    "eg_read_game_file_cached": (_I32, [C.c_char_p, C.POINTER(EgReadOpts), C.c_char_p,
+                                        C.POINTER(C.POINTER(EgOwnedGame))]),
     "eg_parse_text": (_I32, [C.c_char_p, C.c_size_t, _P]),
     "eg_read_file_bytes": (_I32, [C.c_char_p, C.POINTER(C.c_void_p), C.POINTER(C.c_size_t)]),
     "eg_generate": (_I32, [_I32, _I32, _I32, _I32, _I32, C.c_uint64, C.POINTER(C.POINTER(EgOwnedGame))]),
@@ -218,6 +236,10 @@ SIGNATURES = {
     "eg_batch_device_bytes": (_I64, [_P]),
     "eg_batch_free": (None, [_P]),
     "eg_csr2csc_device_noalloc": (_I32, [_I32, _I32, _I64, _P, _P, _P, _P, _P, _P, _P]),
+    "eg_fixture_clique_text": (_I32, [_I32, C.POINTER(C.c_void_p), C.POINTER(C.c_size_t)]),
+    "eg_fixture_ladder_text": (_I32, [_I32, C.POINTER(C.c_void_p), C.POINTER(C.c_size_t)]),
+    "eg_fixture_copies_text": (_I32, [C.c_char_p, C.c_size_t, _I32, C.POINTER(C.c_void_p), C.POINTER(C.c_size_t)]),
+    "eg_free_text": (None, [C.c_void_p]),
     "eg_serve_create": (_I32, [C.POINTER(EgServeOpts), C.POINTER(_P)]),
     "eg_serve_add_game": (_I32, [_P, C.POINTER(EgGame), C.POINTER(_I64)]),
     "eg_serve_remove_game": (_I32, [_P, _I64]),
@@ -226,6 +248,7 @@ SIGNATURES = {
     "eg_serve_wait": (_I32, [_P, _I64, C.c_double]),
     "eg_serve_result": (_I32, [_P, _I64, _P, C.POINTER(_I64)]),
     "eg_serve_stats_get": (_I32, [_P, C.POINTER(EgServeStats)]),
+    "eg_serve_trace": (_I32, [_P, C.POINTER(EgServeSpan), _I32, C.POINTER(_I32)]),
     "eg_serve_destroy": (_I32, [_P]),
 }
 

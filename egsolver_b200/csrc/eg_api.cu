@@ -16,6 +16,9 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <map>
+#include <mutex>
+#include <string>
 #include <vector>
 
 using namespace eg;
@@ -199,8 +202,8 @@ static eg_status check_lanes(const eg_opts *o)
         return eg_set_error(EG_ERR_INVALID, "credit_bits must be 32 or 64 (got %d)", o->credit_bits);
     if (o && (o->direction < EG_DIRECTION_SWITCH || o->direction > EG_DIRECTION_DENSE))
         return eg_set_error(EG_ERR_INVALID, "unknown direction %d", o->direction);
-    if (o && (o->dense_sweeps < 0 || o->dense_sweeps > 2))
-        return eg_set_error(EG_ERR_INVALID, "dense_sweeps must be 0, 1 or 2 (got %d)", o->dense_sweeps);
+    if (o && (o->dense_sweeps < 0 || o->dense_sweeps > kMaxDenseSweeps))
+        return eg_set_error(EG_ERR_INVALID, "dense_sweeps must be in [0, %d] (got %d)", kMaxDenseSweeps, o->dense_sweeps);
     if (o && (o->dense_depth < 0 || o->dense_depth > 2))
         return eg_set_error(EG_ERR_INVALID, "dense_depth must be 0, 1 or 2 (got %d)", o->dense_depth);
     if (o && (o->dense_permille < 0 || o->dense_permille > 1000 || o->sparse_permille < 0 || o->sparse_permille > 1000))
@@ -316,8 +319,9 @@ static eg_status dgame_alloc(const eg_game *game, const eg_opts *opts, eg_dgame 
     if (s == EG_OK) s = dalloc(g, &g->d_PM, (size_t)(g->m_pad_cap / 2 + 64));
     if (s == EG_OK) s = dalloc(g, &g->d_CB, (size_t)(g->m_pad_cap / 64 + 4));
     if (s == EG_OK) s = dalloc(g, &g->d_merr, 1);
-    if (s == EG_OK) s = dalloc(g, &g->d_drem, 2 * (size_t)g->n_pad_cap); /* one bank per sweep */
-    if (s == EG_OK) s = dalloc(g, (int64_t **)&g->d_dacc, 2 * (size_t)g->n_pad_cap);
+    /* one bank of cut-vertex accumulators per sweep of a dense round */
+    if (s == EG_OK) s = dalloc(g, &g->d_drem, (size_t)kMaxDenseSweeps * (size_t)g->n_pad_cap);
+    if (s == EG_OK) s = dalloc(g, (int64_t **)&g->d_dacc, (size_t)kMaxDenseSweeps * (size_t)g->n_pad_cap);
     if (s == EG_OK) s = dalloc(g, &g->d_E8, (size_t)(g->m_pad_cap / 2 + 64));
     if (s != EG_OK) {
         eg_dgame_free(g);
@@ -574,8 +578,10 @@ extern "C" eg_status eg_dgame_solve(eg_dgame *g, const eg_opts *opts_in, eg_stat
         }
     }
     p.nclasses = nc;
-    p.lean = tasks && (opts->variant == EG_VARIANT_AUTO || opts->variant == EG_VARIANT_SMEM) && opts->ctas_per_sm != 2 &&
-             opts->small_max_deg <= 0; /* the lean kernel knows only light words and tasks */
+    /* the lean kernel knows only light words and tasks (a game without a
+     * heavy vertex has no tasks and runs light words alone) */
+    p.lean = !small && (opts->variant == EG_VARIANT_AUTO || opts->variant == EG_VARIANT_SMEM) && opts->ctas_per_sm != 2 &&
+             opts->small_max_deg <= 0;
     /* round kinds: the lean layout alternates frontier rounds (k_lift) and
      * dense rounds (k_lift_dense) */
     const bool kinds = p.lean && g->meta_ok && opts->direction != EG_DIRECTION_SPARSE;
@@ -600,7 +606,7 @@ extern "C" eg_status eg_dgame_solve(eg_dgame *g, const eg_opts *opts_in, eg_stat
     if (kinds) {
         /* one slice of the pair stream per warp of the dense grid */
         p.dense_depth = opts->dense_depth == 1 ? 1 : 2;
-        p.dense_sweeps = opts->dense_sweeps == 1 ? 1 : 2;
+        p.dense_sweeps = opts->dense_sweeps ? opts->dense_sweeps : 2;
         EG_TRY(dense_grid(bits, p.dense_depth, opts->grid_ctas, &dgrid));
         const long long warps = (long long)dgrid * 16;
         const long long per = (g->npairs + warps - 1) / warps;
@@ -881,4 +887,125 @@ extern "C" eg_status eg_cancel_flag_alloc(volatile int32_t **flag)
 extern "C" void eg_cancel_flag_free(volatile int32_t *flag)
 {
     if (flag) cudaFreeHost((void *)flag);
+}
+
+/* ------------------------------------------------------------------ */
+/* Autotuner of the single-game layout                                  */
+/* ------------------------------------------------------------------ */
+
+namespace {
+
+/* Shape of a game for the tuner's cache: log2 of n and of the mean
+ * out-degree, and the share (in 1/16) of vertices in each log2 out-degree
+ * bucket. */
+std::string shape_key(const std::vector<long long> &rp, int n, long long m)
+{
+    int hist[32] = {0};
+    for (int v = 0; v < n; v++) {
+        const long long d = rp[(size_t)v + 1] - rp[(size_t)v];
+        int b = 0;
+        while (b < 31 && (1LL << (b + 1)) <= d) b++;
+        hist[b]++;
+    }
+    std::string key = std::to_string(bits_for(n)) + "/" + std::to_string(bits_for(m / std::max(1, n))) + ":";
+    for (int b = 0; b < 32; b++) key += std::to_string((hist[b] * 16 + n / 2) / std::max(1, n)) + ",";
+    return key;
+}
+
+std::mutex g_tune_mu;
+std::map<std::string, eg_opts> g_tune_cache;
+
+}  // namespace
+
+extern "C" eg_status eg_dgame_tune(eg_dgame *g, const eg_opts *base_in, int64_t rounds, eg_opts *tuned,
+                                   eg_tune_report *rep)
+{
+    if (!g || !tuned) return eg_set_error(EG_ERR_INVALID, "NULL argument");
+    if (rounds < 1) return eg_set_error(EG_ERR_INVALID, "rounds must be >= 1");
+    eg_opts base;
+    if (base_in) base = *base_in;
+    else eg_opts_default(&base);
+    EG_TRY(check_lanes(&base));
+    if (base.variant != EG_VARIANT_AUTO) return eg_set_error(EG_ERR_INVALID, "the tuner tunes the AUTO layout");
+    EG_CUDA(cudaSetDevice(g->device));
+    std::vector<long long> rp((size_t)g->n + 1);
+    EG_CUDA(cudaMemcpy(rp.data(), g->d_rowptr, sizeof(long long) * rp.size(), cudaMemcpyDeviceToHost));
+    const std::string key = shape_key(rp, g->n, g->m) + "|" + std::to_string(base.credit_bits) + "|" +
+                            std::to_string(base.narrow);
+    eg_tune_report r;
+    memset(&r, 0, sizeof r);
+    {
+        std::lock_guard<std::mutex> lk(g_tune_mu);
+        auto it = g_tune_cache.find(key);
+        if (it != g_tune_cache.end()) {
+            eg_opts t = base;
+            const eg_opts &c = it->second;
+            t.large_min_deg = c.large_min_deg;
+            t.small_max_deg = c.small_max_deg;
+            t.task_edges = c.task_edges;
+            t.dense_sweeps = c.dense_sweeps;
+            t.dense_depth = c.dense_depth;
+            *tuned = t;
+            r.from_cache = 1;
+            if (rep) *rep = r;
+            return EG_OK;
+        }
+    }
+    /* coordinate descent: one knob at a time, each candidate a capped solve
+     * from f = 0; the rate is edge relaxations per ms of the lifting loop */
+    auto rate_of = [&](const eg_opts &o, double *rate) -> eg_status {
+        eg_opts t = o;
+        t.keep_layout = 0;
+        t.max_rounds = rounds;
+        t.profile = 0;
+        eg_stats st;
+        eg_status s = eg_dgame_solve(g, &t, &st);
+        if (s != EG_OK && s != EG_ERR_LOOPCAP) return s;
+        *rate = st.lift_ms > 0 ? (double)st.edges / st.lift_ms : 0.0;
+        r.candidates++;
+        return EG_OK;
+    };
+    eg_opts cur = base;
+    /* the defaults spelled out, so that a knob's default is not timed twice */
+    if (cur.large_min_deg <= 1) cur.large_min_deg = 17;
+    if (cur.task_edges <= 0) cur.task_edges = 2 * kTaskPairs;
+    if (cur.dense_sweeps <= 0) cur.dense_sweeps = 2;
+    if (cur.dense_depth <= 0) cur.dense_depth = 2;
+    double best = 0.0;
+    EG_TRY(rate_of(cur, &best));
+    r.default_rate = best;
+    struct Knob {
+        int32_t eg_opts::*field;
+        std::vector<int32_t> values;
+    };
+    const Knob knobs[] = {
+        {&eg_opts::large_min_deg, {9, 17, 33, 65, 129}},   /* light / heavy bound        */
+        {&eg_opts::task_edges, {64, 128, 256}},            /* edges per heavy task       */
+        {&eg_opts::small_max_deg, {0, 2, 4}},              /* thread-per-vertex bucket   */
+        {&eg_opts::dense_sweeps, {1, 2, 3, 4}},            /* sweeps per dense round     */
+        {&eg_opts::dense_depth, {1, 2}},                   /* chunks in flight per warp  */
+    };
+    for (const Knob &k : knobs) {
+        for (int32_t v : k.values) {
+            if (cur.*(k.field) == v) continue;
+            eg_opts cand = cur;
+            cand.*(k.field) = v;
+            double rate = 0.0;
+            EG_TRY(rate_of(cand, &rate));
+            if (rate > best * 1.02) { /* a clear win only: timings have noise */
+                best = rate;
+                cur = cand;
+            }
+        }
+    }
+    r.best_rate = best;
+    cur.max_rounds = base.max_rounds;
+    cur.keep_layout = 0;
+    {
+        std::lock_guard<std::mutex> lk(g_tune_mu);
+        g_tune_cache[key] = cur;
+    }
+    *tuned = cur;
+    if (rep) *rep = r;
+    return EG_OK;
 }

@@ -2,30 +2,45 @@
  * eg_batch.cu -- batched solving of many games at K mean-payoff thresholds
  * in one persistent launch.
  *
- * Layout: the games are packed into one device-resident multi-CSR (global
- * vertex ids, no edge crosses games), with one CSC built by the same stable
- * counting sort as the single-game path.  Credits are stored vertex-major
- * with the K thresholds contiguous, f[(v * K) + k], so the K lanes that
- * lift vertex v for the K thresholds read one successor's K credits as a
- * single contiguous row.
+ * Work is cut into units: a game at a group of 1, 2, 4 or 8 of its
+ * thresholds (weights w * d - p_k).  One CTA solves one unit at a time,
+ * taking units from a device queue, heaviest first.  The unit's credits live
+ * in the CTA's shared memory (rows x group x 4 or 8 bytes, up to the 227 KB
+ * opt-in), so every credit gather of the lift is a shared-memory load; only
+ * games too large for that keep their credits in a global scratch block.
+ * The edges stream from L2 in the sliced layout of eg_batch.cuh, one
+ * coalesced 128-byte column per warp step.
  *
- * Kernel: every CTA takes a game from a device queue (largest games first),
- * computes MG_k = sum_v max(0, p_k - d * min_w(v)), then runs dense rounds
- * of that game alone with CTA barriers: every vertex lifted at every
- * threshold per round, eight independent credit gathers in flight per lane.
- * Mean-payoff threshold games take thousands of rounds in which most
- * vertices rise, so a frontier would hold nearly every vertex anyway.  The
- * lift of vertex v for threshold k is the reference's (reference
- * src/dev_EG_alg.cu:84-109) on the weights w * d - p_k.  No wait in this
- * kernel spins: rounds end at __syncthreads and games come from an atomic
- * counter.
+ * A unit runs in-place sweeps over its vertices (a warp lifts the 32
+ * vertices of a slice for all thresholds of the group at once) until a
+ * sweep raises nothing.  A threshold whose credits did not rise in a sweep
+ * is at its fixed point and is dropped from the following sweeps.  Every
+ * lift reads credits that are initial values or values raised since, all
+ * below the least fixed point, so each threshold's iteration is a fair
+ * chaotic iteration of the reference's lifting operator (reference
+ * src/dev_EG_alg.cu:84-109 on the weights w * d - p, OMINUS of
+ * src/common.h:270-272) and its credits equal the worklist solver's.
+ *
+ * Arithmetic.  For a successor credit a and weight b = w * d - p, OMINUS is
+ * g(a - b) with g(x) = x > MG ? TOP : max(x, 0), TOP stored as 2^30 (32-bit
+ * credits) or 2^62 (64-bit): with MG + wpad * d + |p| below it, a TOP
+ * successor gives a - b > MG, so g maps it to TOP exactly as OMINUS does.
+ * g is monotone, so min_e g(a_e - b_e) = g(p + min_e (a_e - w_e d)) and
+ * likewise for max: per edge and threshold one subtraction and one min (or
+ * max), and g once per vertex.
+ *
+ * No wait in this kernel spins: sweeps end at __syncthreads and units come
+ * from an atomic counter.
  */
 #include "eg_batch.cuh"
 
 #include <algorithm>
+#include <atomic>
 #include <cstdio>
 #include <cstring>
 #include <numeric>
+#include <thread>
+#include <type_traits>
 #include <vector>
 
 using namespace eg;
@@ -46,379 +61,709 @@ using namespace eg;
 
 namespace {
 
-/* OMINUS on 64-bit credits for the weight b = w * d - p (reference
- * src/common.h:270-272); the difference is formed without overflow and only
- * used when a is finite. */
-__device__ __forceinline__ long long ominus64(long long a, long long b, long long mg)
+template <typename CT> struct Lim;
+template <> struct Lim<int> {
+    static constexpr int top = 1 << 30;
+    static constexpr int low = -(1 << 30);
+    static constexpr int lo_acc = INT32_MIN;
+    static constexpr int hi_acc = INT32_MAX;
+};
+template <> struct Lim<long long> {
+    static constexpr long long top = 1LL << 62;
+    static constexpr long long low = -(1LL << 62);
+    static constexpr long long lo_acc = INT64_MIN;
+    static constexpr long long hi_acc = INT64_MAX;
+};
+
+/* The KG credits of one vertex, loaded as one vector. */
+template <int KG, typename CT>
+struct alignas(sizeof(CT) * KG >= 16 ? 16 : sizeof(CT) * KG) Row {
+    CT v[KG];
+};
+
+template <bool WIDE> struct Slot;
+template <> struct Slot<false> {
+    using T = uint32_t;
+    static __device__ __forceinline__ T load(const void *E, int i) { return __ldg((const uint32_t *)E + i); }
+    static __device__ __forceinline__ void dec(T e, int &s, int &w)
+    {
+        s = (int)(e & 0xffffu);
+        w = (int)e >> 16;
+    }
+};
+template <> struct Slot<true> {
+    using T = int2;
+    static __device__ __forceinline__ T load(const void *E, int i) { return __ldg((const int2 *)E + i); }
+    static __device__ __forceinline__ void dec(T e, int &s, int &w)
+    {
+        s = e.x;
+        w = e.y;
+    }
+};
+
+struct Shared {
+    unsigned raise[3];    /* per-sweep OR of raised thresholds (rotating)     */
+    int unit;
+    long long p[8], mg[8];
+};
+
+template <int KG> struct Log2 {
+    static constexpr int v = KG == 1 ? 0 : KG == 2 ? 1 : KG == 4 ? 2 : 3;
+};
+
+/* min (player 0) or max (player 1, MAXV) over the W columns of a slice of
+ * credit - w * d, for the KG thresholds at once; lane's first slot at i0. */
+template <int KG, typename CT, bool WIDE, bool MAXV, int UNR>
+__device__ __forceinline__ void column_walk(const void *E, int i0, int W, const CT *F, CT d, CT (&acc)[KG])
 {
-    const long long t = (long long)INT64_MAX;
-    const long long x = (long long)((unsigned long long)a - (unsigned long long)b);
-    return (a < t && x <= mg) ? (x > 0 ? x : 0) : t;
+    using S = Slot<WIDE>;
+    using ST = typename S::T;
+    using R = Row<KG, CT>;
+    constexpr int LK = Log2<KG>::v;
+#pragma unroll
+    for (int k = 0; k < KG; k++) acc[k] = MAXV ? Lim<CT>::lo_acc : Lim<CT>::hi_acc;
+    for (int c = 0; c < W; c += UNR) {
+        ST q[UNR];
+#pragma unroll
+        for (int x = 0; x < UNR; x++)
+            if (c + x < W) q[x] = S::load(E, i0 + 32 * (c + x));
+        R fr[UNR];
+        int wt[UNR];
+#pragma unroll
+        for (int x = 0; x < UNR; x++) {
+            if (c + x < W) {
+                int sc;
+                S::dec(q[x], sc, wt[x]);
+                fr[x] = *(const R *)(F + ((long long)sc << LK));
+            }
+        }
+#pragma unroll
+        for (int x = 0; x < UNR; x++) {
+            if (c + x < W) {
+                const CT t = (CT)wt[x] * d;
+#pragma unroll
+                for (int k = 0; k < KG; k++) {
+                    const CT y = fr[x].v[k] - t;
+                    acc[k] = MAXV ? (y > acc[k] ? y : acc[k]) : (y < acc[k] ? y : acc[k]);
+                }
+            }
+        }
+    }
 }
 
-/* Edges of a vertex taken together per step of the lift loop: independent
- * credit gathers in flight per lane. */
-constexpr int kBatchUnroll = 8;
-
-/* KP lanes per vertex (KP >= K, a power of two); lane k serves threshold k.
- * Dense rounds: each round lifts every vertex of the game at every
- * threshold in place (no frontier), and the game is solved after a round
- * without a raise.  Every lift reads credits that are the round's start
- * values or values raised since, all below the least fixed point, so this is
- * a fair chaotic iteration of the same operator and the credits equal the
- * worklist solver's. */
-template <int KP>
-__global__ void __launch_bounds__(1024) k_batch_solve(const __grid_constant__ BatchParams p)
+/* Solves one unit (KG thresholds, credit type CT, slot width WIDE, credits
+ * in shared memory or, with GF, in the unit's global scratch). */
+template <int KG, typename CT, bool WIDE, bool GF>
+__device__ __forceinline__ void run_unit(const UnitDesc &u, unsigned char *smem, Shared &sh, const UnitParams &P,
+                                      unsigned long long t0, unsigned long long &lifts, unsigned long long &edges,
+                                      unsigned long long &ntop)
 {
-    __shared__ int s_game;
-    __shared__ long long s_mg[KP];
-    __shared__ int s_p[KP];
-    const int tid = threadIdx.x, lane = tid & 31;
-    const int gl = lane % KP;
-    const int group = tid / KP, ngroups = blockDim.x / KP;
-    const long long TOP = (long long)INT64_MAX;
-    unsigned long long lifts = 0, edges = 0, ntop = 0;
-    if (blockIdx.x == 0 && tid == 0) p.ctrl->t_start = globaltimer_ns();
+    using R = Row<KG, CT>;
+    constexpr CT TOPI = Lim<CT>::top, LOWI = Lim<CT>::low;
+    constexpr int LK = Log2<KG>::v;
+    /* columns whose loads are issued together: about 16 bytes of credits */
+    constexpr int UNR = (KG * (int)sizeof(CT) <= 4) ? 8 : (KG * (int)sizeof(CT) <= 8) ? 4
+                        : (KG * (int)sizeof(CT) <= 16) ? 2 : 1;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nwarps = blockDim.x >> 5;
+    CT *F = GF ? (CT *)u.gscratch : (CT *)smem;
+    const int ns = u.ns, s0 = u.s0, npad = 32 * ns;
+    const int rows = npad + 2;
+    for (int i = tid; i < rows * KG; i += blockDim.x) {
+        const int r = i >> LK;
+        F[i] = r < npad ? (CT)0 : (r == npad ? TOPI : LOWI);
+    }
+    if (tid < KG) {
+        sh.p[tid] = u.p[u.k0 + tid];
+        sh.mg[tid] = u.mg[u.k0 + tid];
+    }
+    if (tid == 0) sh.raise[0] = sh.raise[1] = sh.raise[2] = 0;
+    __syncthreads();
+    const CT d = (CT)u.d;
+    const unsigned full = (1u << KG) - 1u;
+    unsigned amask = full;
+    long long r = 0;
+    int st = EG_OK;
     for (;;) {
-        if (tid == 0) s_game = atomicAdd(&p.ctrl->next_game, 1);
-        __syncthreads();
-        const int gi = s_game;
-        if (gi >= p.num_games) break;
-        const GameDesc gd = p.games[p.order ? p.order[gi] : gi];
-        const long long base = gd.base;
-        const int n = gd.n;
-        const int K = gd.K;
-        const long long d = gd.d;
-        const int *P = gd.P;
-        const int2 *E = gd.E;
-        const unsigned char *owner = gd.owner;
-        long long *F = gd.F - base * K; /* indexed by id * K + k with ids base-relative */
-        if (tid < KP) {
-            s_p[tid] = gd.thr[tid < K ? tid : 0];
-            s_mg[tid] = 0;
-        }
-        for (long long i = tid; i < (long long)n * K; i += blockDim.x) gd.F[i] = 0;
-        __syncthreads();
-        /* MG per threshold: sum_v max(0, p_k - d * min_w(v)) */
-        for (int k = 0; k < K; k++) {
-            long long s = 0;
-            for (int v = tid; v < n; v += blockDim.x) {
-                const long long x = (long long)s_p[k] - (long long)gd.minw[v] * d;
-                s += x > 0 ? x : 0;
-            }
+        unsigned raised = 0;
+        for (int s = warp; s < ns; s += nwarps) {
+            const int b = __ldg(u.slice_off + s);
+            const int W = (__ldg(u.slice_off + s + 1) - b) >> 5;
+            const bool own1 = s >= s0;
+            CT acc[KG];
+            if (own1) column_walk<KG, CT, WIDE, true, UNR>(u.E, b + lane, W, F, d, acc);
+            else column_walk<KG, CT, WIDE, false, UNR>(u.E, b + lane, W, F, d, acc);
+            const int v = 32 * s + lane;
+            const bool real = own1 ? (v - 32 * s0 < u.n1) : (v < u.n0);
+            if (real) {
+                R old = *(const R *)(F + ((long long)v << LK));
 #pragma unroll
-            for (int off = 16; off > 0; off >>= 1) s += __shfl_xor_sync(0xffffffffu, s, off);
-            if (lane == 0 && s) atomicAdd((unsigned long long *)&s_mg[k], (unsigned long long)s);
-        }
-        __syncthreads();
-        const long long pk = s_p[gl];
-        const long long mgk = s_mg[gl];
-        const bool valid = gl < K;
-        long long r = 0;
-        int st = EG_OK;
-        for (;;) {
-            int raised = 0;
-            /* the next vertex's row and owner load while this one is lifted */
-            int eb = 0, ee = 0, own = 0;
-            if (group < n) {
-                eb = P[group];
-                ee = P[group + 1];
-                own = owner[group];
-            }
-            for (int v = group; v < n; v += ngroups) {
-                const long long gv = base + v;
-                const int vn = v + ngroups;
-                int ebn = 0, een = 0, ownn = 0;
-                if (vn < n) {
-                    ebn = P[vn];
-                    een = P[vn + 1];
-                    ownn = owner[vn];
-                }
-                /* only this lane writes F[v][k] in a round: read it early */
-                const long long old = valid ? F[gv * K + gl] : 0;
-                long long acc = own ? 0 : TOP;
-                for (int e = eb; e < ee; e += kBatchUnroll) {
-                    int2 q[kBatchUnroll];
-                    long long f[kBatchUnroll];
-#pragma unroll
-                    for (int j = 0; j < kBatchUnroll; j++)
-                        if (e + j < ee) q[j] = __ldg(E + e + j);
-#pragma unroll
-                    for (int j = 0; j < kBatchUnroll; j++)
-                        f[j] = (valid && e + j < ee) ? F[(long long)q[j].x * K + gl] : 0;
-#pragma unroll
-                    for (int j = 0; j < kBatchUnroll; j++) {
-                        if (valid && e + j < ee) {
-                            const long long val = ominus64(f[j], (long long)q[j].y * d - pk, mgk);
-                            acc = own ? (val > acc ? val : acc) : (val < acc ? val : acc);
+                for (int k = 0; k < KG; k++) {
+                    if (amask >> k & 1u) {
+                        /* threshold and MG from shared memory: used once per vertex */
+                        const CT val = acc[k] + (CT)sh.p[k];
+                        const CT nv = val > (CT)sh.mg[k] ? TOPI : (val > 0 ? val : (CT)0);
+                        if (nv > old.v[k]) {
+                            F[((long long)v << LK) + k] = nv;
+                            raised |= 1u << k;
                         }
                     }
                 }
-                if (valid && old < acc) {
-                    F[gv * K + gl] = acc;
-                    raised = 1;
-                }
-                if (gl == 0) {
-                    lifts++;
-                    edges += (unsigned long long)(ee - eb) * (unsigned long long)K;
-                }
-                eb = ebn;
-                ee = een;
-                own = ownn;
-            }
-            r++;
-            if (!__syncthreads_or(raised)) break;
-            if (p.max_rounds >= 0 && r >= p.max_rounds) {
-                st = EG_ERR_LOOPCAP;
-                break;
-            }
-            const int late = __syncthreads_or(tid == 0 && p.timeout_ns &&
-                                              globaltimer_ns() - p.ctrl->t_start > p.timeout_ns);
-            if (late) {
-                st = EG_ERR_TIMEOUT;
-                break;
             }
         }
-        /* TOP count of this game (all thresholds) */
-        for (long long i = tid; i < (long long)n * K; i += blockDim.x) ntop += (gd.F[i] == TOP);
-        if (tid == 0) {
-            *gd.rounds = r;
-            *gd.status = st;
-        }
+        raised = __reduce_or_sync(0xffffffffu, raised);
+        const int slot = (int)(r % 3);
+        if (lane == 0 && raised) atomicOr(&sh.raise[slot], raised);
+        if (tid == 0 && P.timeout_ns && globaltimer_ns() - t0 > P.timeout_ns) atomicOr(&sh.raise[slot], 1u << 16);
         __syncthreads();
+        const unsigned word = sh.raise[slot];
+        if (tid == 0) {
+            sh.raise[(r + 2) % 3] = 0;
+            lifts += (unsigned long long)(u.n0 + u.n1) * (unsigned)__popc(amask);
+            edges += (unsigned long long)u.m * (unsigned)__popc(amask);
+        }
+        r++;
+        amask &= word & full;
+        if (amask == 0) break;
+        if (word >> 16) {
+            st = EG_ERR_TIMEOUT;
+            break;
+        }
+        if (P.max_rounds >= 0 && r >= P.max_rounds) {
+            st = EG_ERR_LOOPCAP;
+            break;
+        }
     }
-#pragma unroll
-    for (int off = 16; off > 0; off >>= 1) {
-        lifts += __shfl_xor_sync(0xffffffffu, lifts, off);
-        edges += __shfl_xor_sync(0xffffffffu, edges, off);
-        ntop += __shfl_xor_sync(0xffffffffu, ntop, off);
+    __syncthreads();
+    /* credits out, threshold-major in original vertex ids */
+    unsigned long long top = 0;
+    for (int i = tid; i < npad * KG; i += blockDim.x) {
+        const int k = i / npad, v = i - k * npad;
+        const int o = __ldg(u.orig + v);
+        if (o >= 0) {
+            const CT c = F[((long long)v << LK) + k];
+            u.F[(long long)(u.k0 + k) * u.n + o] = c >= TOPI ? (long long)INT64_MAX : (long long)c;
+            top += c >= TOPI;
+        }
     }
-    if (lane == 0) {
-        atomicAdd(&p.ctrl->lifts, lifts);
-        atomicAdd(&p.ctrl->edges, edges);
-        atomicAdd(&p.ctrl->num_top, ntop);
+    ntop += top;
+    if (tid == 0) {
+        *u.rounds = r;
+        *u.status = st;
     }
+    __syncthreads();
 }
 
-}  // namespace
-
-namespace eg {
-
-/* one warp per vertex of the packed graph: CSC sort input and in-degrees */
-__global__ void k_batch_expand(long long total_nodes, const int *P, const int2 *E, int *key, int *val, int *indeg)
+/* One persistent kernel per unit variant: CTAs take units of that variant
+ * from its queue (heaviest first) until it is empty. */
+template <int KG, typename CT, bool WIDE, bool GF>
+__global__ void __launch_bounds__(1024, 1) k_units(const __grid_constant__ UnitParams P)
 {
+    extern __shared__ __align__(16) unsigned char smem[];
+    __shared__ Shared sh;
+    const unsigned long long t0 = globaltimer_ns(); /* this CTA's start */
+    if (threadIdx.x == 0) atomicCAS(&P.ctrl->t_begin, 0ull, t0);
+    unsigned long long lifts = 0, edges = 0, ntop = 0;
+    for (;;) {
+        if (threadIdx.x == 0) sh.unit = atomicAdd(&P.ctrl->next, 1);
+        __syncthreads();
+        const int ui = sh.unit;
+        __syncthreads();
+        if (ui >= P.num_units) break;
+        const UnitDesc u = P.units[ui];
+        run_unit<KG, CT, WIDE, GF>(u, smem, sh, P, t0, lifts, edges, ntop);
+    }
     const int lane = threadIdx.x & 31;
-    const long long w0 = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const long long nw = ((long long)gridDim.x * blockDim.x) >> 5;
-    for (long long v = w0; v < total_nodes; v += nw) {
-        for (int e = P[v] + lane; e < P[v + 1]; e += 32) {
-            const int s = E[e].x;
-            key[e] = s;
-            val[e] = (int)v;
-            atomicAdd(&indeg[s], 1);
-        }
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) ntop += __shfl_xor_sync(0xffffffffu, ntop, off);
+    if (lane == 0 && ntop) atomicAdd(&P.ctrl->num_top, ntop);
+    if (threadIdx.x == 0) {
+        atomicAdd(&P.ctrl->lifts, lifts);
+        atomicAdd(&P.ctrl->edges, edges);
+        atomicMax(&P.ctrl->t_end, globaltimer_ns());
     }
 }
 
-size_t layout_bytes(int n, long long m)
-{
-    return sizeof(int) * ((size_t)n + 1) * 2 + sizeof(int) * (size_t)m + sizeof(int2) * (size_t)m + (size_t)n +
-           2 * sizeof(int) * (size_t)n + 4096;
-}
+typedef void (*unit_kernel_t)(UnitParams);
 
-size_t layout_build_bytes(int n, long long m)
+/* The kernel of a variant (NULL for combinations that do not exist). */
+unit_kernel_t kernel_of(int v)
 {
-    return sizeof(int) * 4 * (size_t)(m + 1) + sizeof(int) * (size_t)(radix_scratch_ints(m) + scan_scratch_ints(n + 1) + 64);
-}
-
-void layout_free(GameLayout *l, cudaStream_t st)
-{
-    void *ptrs[] = {l->P, l->CP, l->CS, l->minw, l->maxw, l->E, l->owner};
-    for (void *q : ptrs)
-        if (q) cudaFreeAsync(q, st);
-    memset(l, 0, sizeof *l);
-}
-
-eg_status layout_upload(const eg_game &G, cudaStream_t st, GameLayout *out)
-{
-    GameLayout L;
-    memset(&L, 0, sizeof L);
-    const int n = G.num_nodes;
-    const long long m = G.num_edges;
-    L.n = n;
-    L.m = m;
-    std::vector<int> P((size_t)n + 1), minw((size_t)n), maxw((size_t)n);
-    std::vector<int2> E((size_t)m);
-    std::vector<unsigned char> own((size_t)n);
-    for (int v = 0; v < n; v++) {
-        P[(size_t)v] = (int)G.row_ptr[v];
-        own[(size_t)v] = G.owner ? G.owner[v] : (unsigned char)(v >= G.num_nodes0);
-        int mn = INT32_MAX, mx = INT32_MIN;
-        for (long long j = G.row_ptr[v]; j < G.row_ptr[v + 1]; j++) {
-            E[(size_t)j] = make_int2(G.succ[j], G.weight[j]);
-            mn = std::min(mn, G.weight[j]);
-            mx = std::max(mx, G.weight[j]);
-        }
-        minw[(size_t)v] = mn;
-        maxw[(size_t)v] = mx;
+#define EG_K(KG, CT, WD, GF) (unit_kernel_t)k_units<KG, CT, WD, GF>
+    switch (v) {
+    case 0: return EG_K(1, int, false, false);
+    case 1: return EG_K(2, int, false, false);
+    case 2: return EG_K(4, int, false, false);
+    case 3: return EG_K(8, int, false, false);
+    case kUnitCredit64 | 0: return EG_K(1, long long, false, false);
+    case kUnitCredit64 | 1: return EG_K(2, long long, false, false);
+    case kUnitCredit64 | 2: return EG_K(4, long long, false, false);
+    case kUnitCredit64 | 3: return EG_K(8, long long, false, false);
+    case kUnitWide | 0: return EG_K(1, int, true, false);
+    case kUnitWide | 1: return EG_K(2, int, true, false);
+    case kUnitWide | 2: return EG_K(4, int, true, false);
+    case kUnitWide | 3: return EG_K(8, int, true, false);
+    case kUnitWide | kUnitCredit64 | 0: return EG_K(1, long long, true, false);
+    case kUnitWide | kUnitCredit64 | 1: return EG_K(2, long long, true, false);
+    case kUnitWide | kUnitCredit64 | 2: return EG_K(4, long long, true, false);
+    case kUnitWide | kUnitCredit64 | 3: return EG_K(8, long long, true, false);
+    case kUnitGlobal: return EG_K(1, int, false, true);
+    case kUnitGlobal | kUnitCredit64: return EG_K(1, long long, false, true);
+    case kUnitGlobal | kUnitWide: return EG_K(1, int, true, true);
+    case kUnitGlobal | kUnitWide | kUnitCredit64: return EG_K(1, long long, true, true);
+    default: return nullptr;
     }
-    P[(size_t)n] = (int)m;
-    cudaError_t e = cudaSuccess;
-    /* stream-ordered allocations: no device-wide synchronisation, so kernels
-     * already running on other streams keep running during an upload */
-#define LA(ptr, cnt)                                                         \
-    if (e == cudaSuccess) {                                                  \
-        e = cudaMallocAsync((void **)&ptr, std::max<size_t>(sizeof(*ptr) * (size_t)(cnt), 16), st); \
-    }
-    LA(L.P, n + 1);
-    LA(L.CP, n + 1);
-    LA(L.CS, m);
-    LA(L.E, m);
-    LA(L.owner, n);
-    LA(L.minw, n);
-    LA(L.maxw, n);
-    int *k0 = nullptr, *v0 = nullptr, *k1 = nullptr, *v1 = nullptr, *scr = nullptr;
-    LA(k0, m + 1);
-    LA(v0, m + 1);
-    LA(k1, m + 1);
-    LA(v1, m + 1);
-    LA(scr, radix_scratch_ints(m) + scan_scratch_ints((long long)n + 1) + 64);
-#undef LA
-    if (e == cudaSuccess) e = cudaMemcpyAsync(L.P, P.data(), sizeof(int) * ((size_t)n + 1), cudaMemcpyHostToDevice, st);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(L.E, E.data(), sizeof(int2) * (size_t)m, cudaMemcpyHostToDevice, st);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(L.owner, own.data(), (size_t)n, cudaMemcpyHostToDevice, st);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(L.minw, minw.data(), sizeof(int) * (size_t)n, cudaMemcpyHostToDevice, st);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(L.maxw, maxw.data(), sizeof(int) * (size_t)n, cudaMemcpyHostToDevice, st);
-    if (e == cudaSuccess) e = cudaMemsetAsync(L.CP, 0, sizeof(int) * ((size_t)n + 1), st);
-    if (e == cudaSuccess) {
-        long long gr = ((long long)n * 32 + 255) / 256;
-        if (gr > 148 * 32) gr = 148 * 32;
-        k_batch_expand<<<(unsigned)gr, 256, 0, st>>>(n, L.P, L.E, k0, v0, L.CP);
-        excl_scan(L.CP, (long long)n + 1, scr, st);
-        int *sk, *sv;
-        radix_sort_pairs(k0, v0, k1, v1, m, bits_for(n), scr, st, &sk, &sv);
-        e = cudaMemcpyAsync(L.CS, sv, sizeof(int) * (size_t)m, cudaMemcpyDeviceToDevice, st);
-    }
-    if (k0) cudaFreeAsync(k0, st);
-    if (v0) cudaFreeAsync(v0, st);
-    if (k1) cudaFreeAsync(k1, st);
-    if (v1) cudaFreeAsync(v1, st);
-    if (scr) cudaFreeAsync(scr, st);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
-    if (e != cudaSuccess) {
-        cudaGetLastError();
-        layout_free(&L, st);
-        cudaStreamSynchronize(st);
-        return eg_set_error(e == cudaErrorMemoryAllocation ? EG_ERR_OOM : EG_ERR_CUDA, "game upload failed: %s",
-                            cudaGetErrorString(e));
-    }
-    L.bytes = layout_bytes(n, m);
-    *out = L;
-    return EG_OK;
+#undef EG_K
 }
 
-GameDesc layout_desc(const GameLayout &l, const int *thr, long long *F, long long *rounds, int *status, int K, int d)
-{
-    GameDesc D;
-    memset(&D, 0, sizeof D);
-    D.P = l.P;
-    D.E = l.E;
-    D.CP = l.CP;
-    D.CS = l.CS;
-    D.owner = l.owner;
-    D.minw = l.minw;
-    D.maxw = l.maxw;
-    D.thr = thr;
-    D.F = F;
-    D.rounds = rounds;
-    D.status = status;
-    D.base = 0;
-    D.n = l.n;
-    D.K = K;
-    D.d = d;
-    return D;
-}
-
-}  // namespace eg
-
-namespace {
+int align32i(int x) { return (x + 31) & ~31; }
 
 }  // namespace
+
+/* ------------------------------------------------------------------ */
+/* Packing, planning and launch (shared with the serving loop)          */
+/* ------------------------------------------------------------------ */
 
 namespace eg {
 
-typedef void (*batch_kernel_t)(BatchParams);
-
-batch_kernel_t kernel_for(int kp)
+eg_status pack_game(const eg_game &G, HostPacked *out)
 {
-    switch (kp) {
-    case 1: return k_batch_solve<1>;
-    case 2: return k_batch_solve<2>;
-    case 4: return k_batch_solve<4>;
-    case 8: return k_batch_solve<8>;
-    case 16: return k_batch_solve<16>;
-    default: return k_batch_solve<32>;
+    HostPacked h;
+    const int n = G.num_nodes;
+    h.n = n;
+    h.m = G.num_edges;
+    auto owner = [&](int v) { return G.owner ? (int)G.owner[v] : (v >= G.num_nodes0 ? 1 : 0); };
+    std::vector<int> deg((size_t)n);
+    long long maxabs = 0;
+    h.minw.assign((size_t)n, 0);
+    for (int v = 0; v < n; v++) {
+        deg[(size_t)v] = (int)(G.row_ptr[v + 1] - G.row_ptr[v]);
+        h.maxdeg = std::max(h.maxdeg, deg[(size_t)v]);
+        int mn = INT32_MAX;
+        for (long long j = G.row_ptr[v]; j < G.row_ptr[v + 1]; j++) {
+            const int w = G.weight[j];
+            mn = std::min(mn, w);
+            maxabs = std::max(maxabs, w < 0 ? -(long long)w : (long long)w);
+        }
+        h.minw[(size_t)v] = mn;
+        if (owner(v)) h.n1++;
+        else h.n0++;
+    }
+    if (maxabs + 1 > (long long)INT32_MAX) return eg_set_error(EG_ERR_INVALID, "weights out of range for the batch path");
+    h.wpad = (int)(maxabs + 1);
+    /* stable counting sort by (owner, degree) */
+    std::vector<int> order((size_t)n);
+    {
+        const int nb = 2 * (h.maxdeg + 1);
+        std::vector<int> cnt((size_t)nb + 1, 0);
+        for (int v = 0; v < n; v++) cnt[(size_t)(owner(v) * (h.maxdeg + 1) + deg[(size_t)v]) + 1]++;
+        for (int i = 0; i < nb; i++) cnt[(size_t)i + 1] += cnt[(size_t)i];
+        for (int v = 0; v < n; v++) order[(size_t)cnt[(size_t)(owner(v) * (h.maxdeg + 1) + deg[(size_t)v])]++] = v;
+    }
+    const int a0 = align32i(h.n0), a1 = align32i(h.n1);
+    const int npad = a0 + a1;
+    h.ns = npad / 32;
+    h.s0 = a0 / 32;
+    h.wide = (npad + 2 > 65536 || h.wpad > 32767) ? 1 : 0;
+    h.orig.assign((size_t)npad, -1);
+    std::vector<int> newid((size_t)n);
+    for (int i = 0; i < n; i++) {
+        const int v = order[(size_t)i];
+        const int u = i < h.n0 ? i : a0 + (i - h.n0);
+        newid[(size_t)v] = u;
+        h.orig[(size_t)u] = v;
+    }
+    h.slice_off.assign((size_t)h.ns + 1, 0);
+    long long slots = 0;
+    for (int s = 0; s < h.ns; s++) {
+        int W = 0;
+        for (int l = 0; l < 32; l++) {
+            const int v = h.orig[(size_t)(32 * s + l)];
+            if (v >= 0) W = std::max(W, deg[(size_t)v]);
+        }
+        slots += 32LL * W;
+        if (slots > (long long)INT32_MAX - 64) return eg_set_error(EG_ERR_INVALID, "game too large for the batch path");
+        h.slice_off[(size_t)s + 1] = (int)slots;
+    }
+    h.slots = slots;
+    const int toprow = npad, lowrow = npad + 1;
+    if (h.wide) h.e64.resize((size_t)slots);
+    else h.e32.resize((size_t)slots);
+    for (int s = 0; s < h.ns; s++) {
+        const int W = (h.slice_off[(size_t)s + 1] - h.slice_off[(size_t)s]) / 32;
+        const bool own1 = s >= h.s0;
+        for (int l = 0; l < 32; l++) {
+            const int v = h.orig[(size_t)(32 * s + l)];
+            for (int j = 0; j < W; j++) {
+                int sc, w;
+                if (v >= 0 && j < deg[(size_t)v]) {
+                    const long long e = G.row_ptr[v] + j;
+                    sc = newid[(size_t)G.succ[e]];
+                    w = G.weight[e];
+                } else {
+                    sc = own1 ? lowrow : toprow;
+                    w = own1 ? h.wpad : -h.wpad;
+                }
+                const size_t at = (size_t)h.slice_off[(size_t)s] + (size_t)j * 32 + (size_t)l;
+                if (h.wide) h.e64[at] = make_int2(sc, w);
+                else h.e32[at] = (uint32_t)(sc & 0xffff) | ((uint32_t)(uint16_t)(int16_t)w << 16);
+            }
+        }
+    }
+    *out = std::move(h);
+    return EG_OK;
+}
+
+static size_t al256(size_t x) { return (x + 255) & ~(size_t)255; }
+
+size_t packed_dev_bytes(const HostPacked &h)
+{
+    const size_t eb = (size_t)h.slots * (h.wide ? sizeof(int2) : sizeof(uint32_t));
+    return al256(std::max<size_t>(eb, 16)) + al256(sizeof(int) * ((size_t)h.ns + 1)) + al256(sizeof(int) * (size_t)(32 * h.ns + 1));
+}
+
+eg_status packed_upload(const HostPacked &h, void *block, cudaStream_t st, PackedDev *out)
+{
+    char *p = (char *)block;
+    const size_t eb = (size_t)h.slots * (h.wide ? sizeof(int2) : sizeof(uint32_t));
+    PackedDev d;
+    d.block = block;
+    d.E = p;
+    d.slice_off = (int *)(p + al256(std::max<size_t>(eb, 16)));
+    d.orig = (int *)((char *)d.slice_off + al256(sizeof(int) * ((size_t)h.ns + 1)));
+    d.bytes = packed_dev_bytes(h);
+    cudaError_t e = cudaSuccess;
+    if (eb) e = cudaMemcpyAsync(d.E, h.wide ? (const void *)h.e64.data() : (const void *)h.e32.data(), eb,
+                                cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(d.slice_off, h.slice_off.data(), sizeof(int) * ((size_t)h.ns + 1), cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess && h.ns)
+        e = cudaMemcpyAsync(d.orig, h.orig.data(), sizeof(int) * (size_t)(32 * h.ns), cudaMemcpyHostToDevice, st);
+    if (e != cudaSuccess) return eg_set_error(EG_ERR_CUDA, "packed game upload failed: %s", cudaGetErrorString(e));
+    *out = d;
+    return EG_OK;
+}
+
+long long threshold_mg(const HostPacked &h, int p, int d)
+{
+    long long s = 0;
+    for (int v = 0; v < h.n; v++) {
+        const long long x = (long long)p - (long long)d * h.minw[(size_t)v];
+        if (x > 0) s += x;
+    }
+    return s;
+}
+
+bool credits32_ok(const HostPacked &h, const int *p, int K, int d, const long long *mg)
+{
+    for (int k = 0; k < K; k++) {
+        const long long ap = p[k] < 0 ? -(long long)p[k] : (long long)p[k];
+        if (mg[k] + (long long)h.wpad * d + ap >= (1LL << 30)) return false;
+    }
+    return true;
+}
+
+UnitPlan plan_game(const HostPacked &h, bool credit64, int smem_budget, int kg_cap)
+{
+    UnitPlan pl;
+    pl.credit64 = credit64 ? 1 : 0;
+    pl.kg_max = 0;
+    const long long cb = credit64 ? 8 : 4;
+    for (int kg = 8; kg >= 1; kg >>= 1) {
+        if (kg > kg_cap) continue;
+        if ((long long)h.rows() * kg * cb <= smem_budget) {
+            pl.kg_max = kg;
+            break;
+        }
+    }
+    return pl;
+}
+
+void split_thresholds(int K, int kg_max, std::vector<std::pair<int, int>> *groups)
+{
+    const int cap = kg_max < 1 ? 1 : kg_max;
+    int k0 = 0;
+    while (k0 < K) {
+        int g = 1;
+        while (g * 2 <= cap && g * 2 <= K - k0) g *= 2;
+        groups->push_back({k0, g == 1 ? 0 : g == 2 ? 1 : g == 4 ? 2 : 3});
+        k0 += g;
     }
 }
 
-eg_status launch_batch(const BatchParams &p, int KP, int block, int num_sms, cudaStream_t st, int *grid_out)
+eg_status make_units(const HostPacked &h, const PackedDev &pd, int K, int d, const int *p, const long long *mg,
+                     const int *p_dev, const long long *mg_dev, long long *F_dev, int smem_budget, int kg_cap,
+                     std::vector<UnitDesc> *units, std::vector<size_t> *gneed, std::vector<long long> *cost,
+                     int *smem)
 {
-    batch_kernel_t fn = kernel_for(KP);
-    const size_t smem = 0; /* dense rounds keep no frontier */
-    int per_sm = 0;
-    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void *)fn, block, smem);
-    if (e != cudaSuccess || per_sm < 1)
-        return eg_set_error(EG_ERR_CUDA, "batch kernel does not fit (block %d, %zu B shared)", block, smem);
-    int grid = num_sms * per_sm;
-    if (grid > p.num_games) grid = p.num_games;
-    if (grid < 1) grid = 1;
-    e = cudaMemsetAsync(p.ctrl, 0, sizeof(BatchCtrl), st);
-    if (e != cudaSuccess) return eg_set_error(EG_ERR_CUDA, "cudaMemsetAsync failed: %s", cudaGetErrorString(e));
-    void *args[] = {(void *)&p};
-    e = cudaLaunchKernel((const void *)fn, dim3(grid), dim3(block), args, smem, st);
-    if (e != cudaSuccess) return eg_set_error(EG_ERR_CUDA, "batch kernel launch failed: %s", cudaGetErrorString(e));
-    *grid_out = grid;
+    if ((long long)h.wpad * d >= (1LL << 31))
+        return eg_set_error(EG_ERR_OVERFLOW, "weight * scale does not fit 32 bits");
+    for (int k = 0; k < K; k++)
+        if (mg[k] >= (1LL << 61)) return eg_set_error(EG_ERR_OVERFLOW, "threshold %d: MG %lld too large", k, mg[k]);
+    const bool c64 = !credits32_ok(h, p, K, d, mg);
+    const UnitPlan pl = plan_game(h, c64, smem_budget, kg_cap);
+    std::vector<std::pair<int, int>> groups;
+    split_thresholds(K, pl.kg_max, &groups);
+    for (auto &gr : groups) {
+        UnitDesc u;
+        memset(&u, 0, sizeof u);
+        u.E = pd.E;
+        u.slice_off = pd.slice_off;
+        u.orig = pd.orig;
+        u.p = p_dev;
+        u.mg = mg_dev;
+        u.F = F_dev;
+        u.m = h.m;
+        u.n = h.n;
+        u.n0 = h.n0;
+        u.n1 = h.n1;
+        u.ns = h.ns;
+        u.s0 = h.s0;
+        u.d = d;
+        u.k0 = gr.first;
+        const int kg = 1 << gr.second;
+        const size_t need = (size_t)h.rows() * kg * (c64 ? 8 : 4);
+        if (pl.kg_max == 0) {
+            u.variant = (c64 ? kUnitCredit64 : 0) | (h.wide ? kUnitWide : 0) | kUnitGlobal;
+            gneed->push_back((need + 255) & ~(size_t)255);
+        } else {
+            u.variant = gr.second | (c64 ? kUnitCredit64 : 0) | (h.wide ? kUnitWide : 0);
+            gneed->push_back(0);
+            *smem = std::max(*smem, (int)need);
+        }
+        units->push_back(u);
+        cost->push_back(h.m * (long long)h.n * kg);
+    }
     return EG_OK;
+}
+
+int unit_smem_budget(int device)
+{
+    int optin = 0;
+    if (cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device) != cudaSuccess) {
+        cudaGetLastError();
+        optin = 48 * 1024;
+    }
+    int stat = 0;
+    for (int v = 0; v < kNumVariants; v++) {
+        unit_kernel_t k = kernel_of(v);
+        if (!k) continue;
+        cudaFuncAttributes fa;
+        memset(&fa, 0, sizeof fa);
+        if (cudaFuncGetAttributes(&fa, (const void *)k) != cudaSuccess) cudaGetLastError();
+        stat = std::max(stat, (int)fa.sharedSizeBytes);
+    }
+    return optin - stat - 64;
+}
+
+eg_status unit_kernel_setup(int device)
+{
+    const int budget = unit_smem_budget(device);
+    for (int v = 0; v < kNumVariants; v++) {
+        unit_kernel_t k = kernel_of(v);
+        if (!k) continue;
+        cudaError_t e = cudaFuncSetAttribute((const void *)k, cudaFuncAttributeMaxDynamicSharedMemorySize, budget);
+        if (e != cudaSuccess) return eg_set_error(EG_ERR_CUDA, "cudaFuncSetAttribute failed: %s", cudaGetErrorString(e));
+    }
+    return EG_OK;
+}
+
+void group_units(const std::vector<UnitDesc> &units, const std::vector<long long> &cost,
+                 const std::vector<size_t> &gneed, UnitSet *out, std::vector<int> *perm)
+{
+    const int nu = (int)units.size();
+    std::vector<int> order((size_t)nu);
+    std::iota(order.begin(), order.end(), 0);
+    std::stable_sort(order.begin(), order.end(), [&](int a, int c) {
+        if (units[(size_t)a].variant != units[(size_t)c].variant)
+            return units[(size_t)a].variant < units[(size_t)c].variant;
+        return cost[(size_t)a] > cost[(size_t)c];
+    });
+    UnitSet S;
+    for (int v = 0; v <= kNumVariants; v++) S.off[v] = 0;
+    for (int v = 0; v < kNumVariants; v++) {
+        S.smem[v] = 16;
+        S.top_cost[v] = -1;
+    }
+    for (int i : order) {
+        const UnitDesc &u = units[(size_t)i];
+        const int v = u.variant;
+        S.units.push_back(u);
+        S.gneed.push_back(gneed[(size_t)i]);
+        S.off[v + 1]++;
+        S.top_cost[v] = std::max(S.top_cost[v], cost[(size_t)i]);
+        if (!(v & kUnitGlobal)) {
+            const int kg = 1 << (v & kUnitKgMask);
+            const int need = (32 * u.ns + 2) * kg * ((v & kUnitCredit64) ? 8 : 4);
+            S.smem[v] = std::max(S.smem[v], need);
+        }
+    }
+    for (int v = 0; v < kNumVariants; v++) S.off[v + 1] += S.off[v];
+    if (perm) *perm = order;
+    *out = std::move(S);
+}
+
+eg_status UnitLauncher::init()
+{
+    if (cudaEventCreateWithFlags(&fork, cudaEventDisableTiming) != cudaSuccess)
+        return eg_set_error(EG_ERR_CUDA, "event creation failed");
+    for (int v = 0; v < kNumVariants; v++) {
+        if (!kernel_of(v)) continue;
+        if (cudaStreamCreateWithFlags(&aux[v], cudaStreamNonBlocking) != cudaSuccess ||
+            cudaEventCreateWithFlags(&join[v], cudaEventDisableTiming) != cudaSuccess)
+            return eg_set_error(EG_ERR_CUDA, "stream creation failed");
+    }
+    return EG_OK;
+}
+
+void UnitLauncher::destroy()
+{
+    for (int v = 0; v < kNumVariants; v++) {
+        if (aux[v]) cudaStreamDestroy(aux[v]);
+        if (join[v]) cudaEventDestroy(join[v]);
+        aux[v] = nullptr;
+        join[v] = nullptr;
+    }
+    if (fork) cudaEventDestroy(fork);
+    fork = nullptr;
+}
+
+eg_status launch_unit_set(UnitLauncher &L, cudaStream_t main, const UnitSet &S, const UnitDesc *units_dev,
+                          UnitCtrl *ctrl_dev, int block, int num_sms, long long max_rounds,
+                          unsigned long long timeout_ns, int *grid_total)
+{
+    cudaError_t e = cudaMemsetAsync(ctrl_dev, 0, sizeof(UnitCtrl) * kNumVariants, main);
+    if (e == cudaSuccess) e = cudaEventRecord(L.fork, main);
+    if (e != cudaSuccess) return eg_set_error(EG_ERR_CUDA, "launch set-up failed: %s", cudaGetErrorString(e));
+    /* the variant holding the heaviest unit is launched first */
+    std::vector<int> vs;
+    for (int v = 0; v < kNumVariants; v++)
+        if (S.off[v + 1] > S.off[v]) vs.push_back(v);
+    std::stable_sort(vs.begin(), vs.end(), [&](int a, int c) { return S.top_cost[a] > S.top_cost[c]; });
+    int total = 0;
+    for (int v : vs) {
+        unit_kernel_t k = kernel_of(v);
+        if (!k) return eg_set_error(EG_ERR_INVALID, "no kernel for unit variant %d", v);
+        int per_sm = 0;
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void *)k, block, (size_t)S.smem[v]);
+        if (e != cudaSuccess || per_sm < 1)
+            return eg_set_error(EG_ERR_CUDA, "unit kernel does not fit (block %d, %d B shared)", block, S.smem[v]);
+        const int count = S.off[v + 1] - S.off[v];
+        const int grid = std::max(1, std::min(num_sms * per_sm, count));
+        UnitParams p;
+        memset(&p, 0, sizeof p);
+        p.units = units_dev + S.off[v];
+        p.ctrl = ctrl_dev + v;
+        p.num_units = count;
+        p.max_rounds = max_rounds;
+        p.timeout_ns = timeout_ns;
+        void *args[] = {(void *)&p};
+        e = cudaStreamWaitEvent(L.aux[v], L.fork, 0);
+        if (e == cudaSuccess) e = cudaLaunchKernel((const void *)k, dim3(grid), dim3(block), args, (size_t)S.smem[v], L.aux[v]);
+        if (e == cudaSuccess) e = cudaEventRecord(L.join[v], L.aux[v]);
+        if (e == cudaSuccess) e = cudaStreamWaitEvent(main, L.join[v], 0);
+        if (e != cudaSuccess) return eg_set_error(EG_ERR_CUDA, "unit kernel launch failed: %s", cudaGetErrorString(e));
+        total += grid;
+    }
+    if (grid_total) *grid_total = total;
+    return EG_OK;
+}
+
+void sum_ctrl(const UnitCtrl *c, UnitCtrl *out)
+{
+    memset(out, 0, sizeof *out);
+    for (int v = 0; v < kNumVariants; v++) {
+        out->lifts += c[v].lifts;
+        out->edges += c[v].edges;
+        out->num_top += c[v].num_top;
+        if (c[v].t_begin && (!out->t_begin || c[v].t_begin < out->t_begin)) out->t_begin = c[v].t_begin;
+        out->t_end = std::max(out->t_end, c[v].t_end);
+    }
 }
 
 }  // namespace eg
 
-namespace {
-
-int pow2_at_least(int k)
-{
-    int x = 1;
-    while (x < k) x <<= 1;
-    return x;
-}
-
-}  // namespace
+/* ------------------------------------------------------------------ */
+/* Batch API                                                            */
+/* ------------------------------------------------------------------ */
 
 struct eg_batch {
-    int device;
-    cudaStream_t st;
-    cudaEvent_t ev0, ev1;
-    int num_games, K, KP, d;
-    long long total_nodes, total_edges;
-    int words_max;
-    int block;
-    long long max_rounds;
-    double timeout_ms;
-    std::vector<long long> node_off_h;
-    long long *node_off;
-    int *order, *P, *CP, *CS, *minw, *maxw, *thr, *status;
-    int2 *E;
-    unsigned char *owner;
-    long long *F, *rounds;
-    BatchCtrl *ctrl;
-    GameDesc *desc;
-    size_t bytes;
-    bool thresholds_set, solved;
-    bool use_graph;
-    cudaGraph_t graph;
-    cudaGraphExec_t graph_exec;
-    int graph_block;
+    int device = 0;
+    cudaStream_t st = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    int num_games = 0, K = 0, d = 1;
+    long long total_nodes = 0, total_edges = 0;
+    int block = 1024, kg_cap = 8, smem_budget = 0, sms = 148;
+    long long max_rounds = -1;
+    double timeout_ms = 0;
+    std::vector<HostPacked> hp;      /* host images (slots dropped after upload) */
+    std::vector<PackedDev> pd;
+    std::vector<long long> f_off;    /* credits of game g start at F + f_off[g]  */
+    void *dblock = nullptr;          /* packed games                             */
+    long long *F = nullptr;          /* sum_g n_g * K credits                    */
+    int *p_dev = nullptr;            /* num_games * K thresholds                 */
+    long long *mg_dev = nullptr;     /* num_games * K MG values                  */
+    std::vector<int> p_host;
+    std::vector<long long> mg_host;
+    UnitSet set;                     /* units grouped by variant                 */
+    std::vector<int> unit_game;      /* game of each grouped unit                */
+    UnitDesc *units_dev = nullptr;
+    long long *u_rounds = nullptr;
+    int *u_status = nullptr;
+    int units_cap = 0;
+    void *gscratch = nullptr;
+    size_t gscratch_bytes = 0;
+    UnitCtrl *ctrl = nullptr;        /* kNumVariants counters                    */
+    UnitLauncher launcher;
+    size_t bytes = 0, unit_bytes = 0;
+    bool thresholds_set = false, solved = false, use_graph = false;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t graph_exec = nullptr;
+    int graph_block = 0, graph_grid = 0;
+    std::vector<long long> last_rounds;
+    std::vector<int> last_status;
 };
+
+static void batch_drop_graph(eg_batch *b)
+{
+    if (b->graph_exec) cudaGraphExecDestroy(b->graph_exec);
+    if (b->graph) cudaGraphDestroy(b->graph);
+    b->graph_exec = nullptr;
+    b->graph = nullptr;
+}
+
+static void batch_free_units(eg_batch *b)
+{
+    void *ptrs[] = {b->units_dev, b->u_rounds, b->u_status, b->gscratch};
+    for (void *q : ptrs)
+        if (q) cudaFree(q);
+    b->units_dev = nullptr;
+    b->u_rounds = nullptr;
+    b->u_status = nullptr;
+    b->gscratch = nullptr;
+    b->gscratch_bytes = 0;
+    b->units_cap = 0;
+    b->bytes -= b->unit_bytes;
+    b->unit_bytes = 0;
+}
+
+extern "C" void eg_batch_free(eg_batch *b)
+{
+    if (!b) return;
+    cudaSetDevice(b->device);
+    if (b->st) cudaStreamSynchronize(b->st);
+    batch_drop_graph(b);
+    batch_free_units(b);
+    void *ptrs[] = {b->dblock, b->F, b->p_dev, b->mg_dev, b->ctrl};
+    for (void *q : ptrs)
+        if (q) cudaFree(q);
+    b->launcher.destroy();
+    if (b->ev0) cudaEventDestroy(b->ev0);
+    if (b->ev1) cudaEventDestroy(b->ev1);
+    if (b->st) cudaStreamDestroy(b->st);
+    delete b;
+}
+
+extern "C" int64_t eg_batch_device_bytes(const eg_batch *b) { return b ? (int64_t)b->bytes : 0; }
 
 template <class T>
 static eg_status balloc(eg_batch *b, T **p, size_t count)
@@ -434,24 +779,24 @@ static eg_status balloc(eg_batch *b, T **p, size_t count)
     return EG_OK;
 }
 
-extern "C" void eg_batch_free(eg_batch *b)
+/* Runs fn(i) for i in [0, count) on the host's cores. */
+template <class Fn>
+static void parallel_for(int count, Fn fn)
 {
-    if (!b) return;
-    cudaSetDevice(b->device);
-    if (b->st) cudaStreamSynchronize(b->st);
-    if (b->graph_exec) cudaGraphExecDestroy(b->graph_exec);
-    if (b->graph) cudaGraphDestroy(b->graph);
-    void *ptrs[] = {b->node_off, b->order, b->P, b->CP, b->CS, b->minw, b->maxw, b->thr,
-                    b->status, b->E, b->owner, b->F, b->rounds, b->ctrl, b->desc};
-    for (void *q : ptrs)
-        if (q) cudaFree(q);
-    if (b->ev0) cudaEventDestroy(b->ev0);
-    if (b->ev1) cudaEventDestroy(b->ev1);
-    if (b->st) cudaStreamDestroy(b->st);
-    delete b;
+    int nt = (int)std::thread::hardware_concurrency();
+    nt = std::max(1, std::min(nt, 32));
+    if (count < 4 || nt == 1) {
+        for (int i = 0; i < count; i++) fn(i);
+        return;
+    }
+    std::vector<std::thread> th;
+    std::atomic<int> next(0);
+    for (int t = 0; t < nt; t++)
+        th.emplace_back([&]() {
+            for (int i = next.fetch_add(1); i < count; i = next.fetch_add(1)) fn(i);
+        });
+    for (auto &x : th) x.join();
 }
-
-extern "C" int64_t eg_batch_device_bytes(const eg_batch *b) { return b ? (int64_t)b->bytes : 0; }
 
 extern "C" eg_status eg_batch_create(const eg_game *games, int32_t num_games, const eg_batch_opts *opts, eg_batch **out)
 {
@@ -461,8 +806,9 @@ extern "C" eg_status eg_batch_create(const eg_game *games, int32_t num_games, co
     if (opts->scale < 1) return eg_set_error(EG_ERR_INVALID, "scale d must be >= 1");
     if (opts->block && (opts->block < 64 || opts->block > 1024 || (opts->block & 31)))
         return eg_set_error(EG_ERR_INVALID, "block must be a multiple of 32 in [64, 1024]");
+    if (opts->group_max && opts->group_max != 1 && opts->group_max != 2 && opts->group_max != 4 && opts->group_max != 8)
+        return eg_set_error(EG_ERR_INVALID, "group_max must be 1, 2, 4 or 8");
     long long tn = 0, tm = 0;
-    int nmax = 0;
     for (int g = 0; g < num_games; g++) {
         eg_status s = eg_validate(&games[g]);
         if (s != EG_OK) return eg_set_error(s, "game %d: %s", g, eg_last_error());
@@ -471,148 +817,143 @@ extern "C" eg_status eg_batch_create(const eg_game *games, int32_t num_games, co
                                 g, games[g].num_nodes, kBatchMaxGameNodes);
         tn += games[g].num_nodes;
         tm += games[g].num_edges;
-        nmax = std::max(nmax, games[g].num_nodes);
     }
-    if (tn >= (long long)INT32_MAX - 64 || tm >= (long long)INT32_MAX - 64)
-        return eg_set_error(EG_ERR_INVALID, "batch too large (%lld vertices, %lld edges)", tn, tm);
     int count = 0;
     if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0) {
         cudaGetLastError();
         return eg_set_error(EG_ERR_NO_DEVICE, "no CUDA device available");
     }
+    if (opts->device < 0 || opts->device >= count) return eg_set_error(EG_ERR_INVALID, "device %d not available", opts->device);
     EG_CUDA(cudaSetDevice(opts->device));
     eg_batch *b = new eg_batch();
     b->device = opts->device;
     b->num_games = num_games;
     b->K = opts->thresholds;
-    b->KP = pow2_at_least(opts->thresholds);
     b->d = opts->scale;
     b->total_nodes = tn;
     b->total_edges = tm;
-    b->words_max = (nmax + 31) / 32;
     b->block = opts->block ? opts->block : 1024;
+    b->kg_cap = opts->group_max ? opts->group_max : 8;
     b->max_rounds = opts->max_rounds;
     b->timeout_ms = opts->timeout_ms;
     b->use_graph = opts->use_graph != 0;
-    /* host packing: global ids, owners, min/max out-weight */
-    std::vector<int> P((size_t)tn + 1), minw((size_t)tn), maxw((size_t)tn);
-    std::vector<int2> E((size_t)tm);
-    std::vector<unsigned char> own((size_t)tn);
-    b->node_off_h.assign((size_t)num_games + 1, 0);
-    long long vb = 0, eb = 0;
-    for (int g = 0; g < num_games; g++) {
-        const eg_game &G = games[g];
-        b->node_off_h[g] = vb;
-        for (int v = 0; v < G.num_nodes; v++) {
-            P[(size_t)(vb + v)] = (int)(eb + G.row_ptr[v]);
-            own[(size_t)(vb + v)] = G.owner ? G.owner[v] : (unsigned char)(v >= G.num_nodes0);
-            int mn = INT32_MAX, mx = INT32_MIN;
-            for (long long j = G.row_ptr[v]; j < G.row_ptr[v + 1]; j++) {
-                const int w = G.weight[j];
-                E[(size_t)(eb + j)] = make_int2((int)(vb + G.succ[j]), w);
-                mn = std::min(mn, w);
-                mx = std::max(mx, w);
-            }
-            minw[(size_t)(vb + v)] = mn;
-            maxw[(size_t)(vb + v)] = mx;
-        }
-        vb += G.num_nodes;
-        eb += G.num_edges;
-    }
-    b->node_off_h[num_games] = vb;
-    P[(size_t)tn] = (int)tm;
-    std::vector<int> order((size_t)num_games);
-    std::iota(order.begin(), order.end(), 0);
-    std::stable_sort(order.begin(), order.end(), [&](int a, int c) { return games[a].num_edges > games[c].num_edges; });
-
-    eg_status s = EG_OK;
-    cudaError_t e = cudaStreamCreateWithFlags(&b->st, cudaStreamNonBlocking);
-    if (e == cudaSuccess) e = cudaEventCreate(&b->ev0);
-    if (e == cudaSuccess) e = cudaEventCreate(&b->ev1);
-    if (e != cudaSuccess) s = eg_set_error(EG_ERR_CUDA, "stream/event creation failed: %s", cudaGetErrorString(e));
-    if (s == EG_OK) s = balloc(b, &b->node_off, (size_t)num_games + 1);
-    if (s == EG_OK) s = balloc(b, &b->order, (size_t)num_games);
-    if (s == EG_OK) s = balloc(b, &b->P, (size_t)tn + 1);
-    if (s == EG_OK) s = balloc(b, &b->CP, (size_t)tn + 1);
-    if (s == EG_OK) s = balloc(b, &b->CS, (size_t)tm);
-    if (s == EG_OK) s = balloc(b, &b->E, (size_t)tm);
-    if (s == EG_OK) s = balloc(b, &b->owner, (size_t)tn);
-    if (s == EG_OK) s = balloc(b, &b->minw, (size_t)tn);
-    if (s == EG_OK) s = balloc(b, &b->maxw, (size_t)tn);
-    if (s == EG_OK) s = balloc(b, &b->thr, (size_t)num_games * b->K);
-    if (s == EG_OK) s = balloc(b, &b->F, (size_t)tn * b->K);
-    if (s == EG_OK) s = balloc(b, &b->rounds, (size_t)num_games);
-    if (s == EG_OK) s = balloc(b, &b->status, (size_t)num_games);
-    if (s == EG_OK) s = balloc(b, &b->ctrl, 1);
-    if (s == EG_OK) s = balloc(b, &b->desc, (size_t)num_games);
+    cudaDeviceGetAttribute(&b->sms, cudaDevAttrMultiProcessorCount, b->device);
+    eg_status s = unit_kernel_setup(b->device);
+    if (s == EG_OK) s = b->launcher.init();
     if (s != EG_OK) {
         eg_batch_free(b);
         return s;
     }
-    /* one descriptor per game, pointing into the packed arrays */
-    std::vector<GameDesc> desc((size_t)num_games);
+    b->smem_budget = unit_smem_budget(b->device);
+    /* pack every game on the host cores */
+    b->hp.resize((size_t)num_games);
+    std::vector<eg_status> ps((size_t)num_games, EG_OK);
+    parallel_for(num_games, [&](int g) { ps[(size_t)g] = pack_game(games[g], &b->hp[(size_t)g]); });
+    for (int g = 0; g < num_games; g++)
+        if (ps[(size_t)g] != EG_OK) {
+            eg_batch_free(b);
+            return eg_set_error(ps[(size_t)g], "game %d could not be packed", g);
+        }
+    size_t pbytes = 0;
+    std::vector<size_t> poff((size_t)num_games);
+    b->f_off.assign((size_t)num_games + 1, 0);
     for (int g = 0; g < num_games; g++) {
-        const long long base = b->node_off_h[g];
-        GameDesc &D = desc[(size_t)g];
-        D.P = b->P + base;
-        D.E = b->E;
-        D.CP = b->CP + base;
-        D.CS = b->CS;
-        D.owner = b->owner + base;
-        D.minw = b->minw + base;
-        D.maxw = b->maxw + base;
-        D.thr = b->thr + (long long)g * b->K;
-        D.F = b->F + base * b->K;
-        D.rounds = b->rounds + g;
-        D.status = b->status + g;
-        D.base = base;
-        D.n = games[g].num_nodes;
-        D.K = b->K;
-        D.d = b->d;
-        D.pad = 0;
+        poff[(size_t)g] = pbytes;
+        pbytes += packed_dev_bytes(b->hp[(size_t)g]);
+        b->f_off[(size_t)g + 1] = b->f_off[(size_t)g] + (long long)b->hp[(size_t)g].n * b->K;
     }
-    cudaStream_t st = b->st;
-    e = cudaMemcpyAsync(b->node_off, b->node_off_h.data(), sizeof(long long) * ((size_t)num_games + 1),
-                        cudaMemcpyHostToDevice, st);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(b->order, order.data(), sizeof(int) * (size_t)num_games, cudaMemcpyHostToDevice, st);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(b->desc, desc.data(), sizeof(GameDesc) * desc.size(), cudaMemcpyHostToDevice, st);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(b->P, P.data(), sizeof(int) * ((size_t)tn + 1), cudaMemcpyHostToDevice, st);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(b->E, E.data(), sizeof(int2) * (size_t)tm, cudaMemcpyHostToDevice, st);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(b->owner, own.data(), (size_t)tn, cudaMemcpyHostToDevice, st);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(b->minw, minw.data(), sizeof(int) * (size_t)tn, cudaMemcpyHostToDevice, st);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(b->maxw, maxw.data(), sizeof(int) * (size_t)tn, cudaMemcpyHostToDevice, st);
-    /* CSC by the stable counting sort, with temporary sort buffers */
-    int *k0 = nullptr, *v0 = nullptr, *k1 = nullptr, *v1 = nullptr, *scr = nullptr;
-    const long long scr_ints = radix_scratch_ints(tm) + scan_scratch_ints(tn + 1) + 64;
-    if (e == cudaSuccess) e = cudaMalloc(&k0, sizeof(int) * (size_t)std::max<long long>(tm, 1));
-    if (e == cudaSuccess) e = cudaMalloc(&v0, sizeof(int) * (size_t)std::max<long long>(tm, 1));
-    if (e == cudaSuccess) e = cudaMalloc(&k1, sizeof(int) * (size_t)std::max<long long>(tm, 1));
-    if (e == cudaSuccess) e = cudaMalloc(&v1, sizeof(int) * (size_t)std::max<long long>(tm, 1));
-    if (e == cudaSuccess) e = cudaMalloc(&scr, sizeof(int) * (size_t)scr_ints);
-    if (e == cudaSuccess) e = cudaMemsetAsync(b->CP, 0, sizeof(int) * ((size_t)tn + 1), st);
-    if (e == cudaSuccess) {
-        long long gr = (tn * 32 + 255) / 256;
-        if (gr > 148 * 32) gr = 148 * 32;
-        k_batch_expand<<<(unsigned)gr, 256, 0, st>>>(tn, b->P, b->E, k0, v0, b->CP);
-        excl_scan(b->CP, tn + 1, scr, st);
-        int *sk, *sv;
-        radix_sort_pairs(k0, v0, k1, v1, tm, bits_for(tn), scr, st, &sk, &sv);
-        e = cudaMemcpyAsync(b->CS, sv, sizeof(int) * (size_t)tm, cudaMemcpyDeviceToDevice, st);
+    cudaError_t e = cudaStreamCreateWithFlags(&b->st, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaEventCreate(&b->ev0);
+    if (e == cudaSuccess) e = cudaEventCreate(&b->ev1);
+    if (e != cudaSuccess) s = eg_set_error(EG_ERR_CUDA, "stream/event creation failed: %s", cudaGetErrorString(e));
+    if (s == EG_OK) s = balloc(b, (char **)&b->dblock, pbytes);
+    if (s == EG_OK) s = balloc(b, &b->F, (size_t)b->f_off[(size_t)num_games]);
+    if (s == EG_OK) s = balloc(b, &b->p_dev, (size_t)num_games * b->K);
+    if (s == EG_OK) s = balloc(b, &b->mg_dev, (size_t)num_games * b->K);
+    if (s == EG_OK) s = balloc(b, &b->ctrl, (size_t)kNumVariants);
+    b->pd.resize((size_t)num_games);
+    for (int g = 0; g < num_games && s == EG_OK; g++)
+        s = packed_upload(b->hp[(size_t)g], (char *)b->dblock + poff[(size_t)g], b->st, &b->pd[(size_t)g]);
+    if (s == EG_OK) {
+        e = cudaStreamSynchronize(b->st);
+        if (e != cudaSuccess) s = eg_set_error(EG_ERR_CUDA, "batch upload failed: %s", cudaGetErrorString(e));
     }
-    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
-    cudaFree(k0);
-    cudaFree(v0);
-    cudaFree(k1);
-    cudaFree(v1);
-    cudaFree(scr);
-    if (e != cudaSuccess) {
-        s = eg_set_error(e == cudaErrorMemoryAllocation ? EG_ERR_OOM : EG_ERR_CUDA, "batch upload failed: %s",
-                         cudaGetErrorString(e));
-        cudaGetLastError();
+    if (s != EG_OK) {
         eg_batch_free(b);
         return s;
     }
+    /* the device holds the slots now; the host keeps sizes and min weights */
+    for (HostPacked &h : b->hp) {
+        std::vector<uint32_t>().swap(h.e32);
+        std::vector<int2>().swap(h.e64);
+        std::vector<int>().swap(h.orig);
+        std::vector<int>().swap(h.slice_off);
+    }
     *out = b;
+    return EG_OK;
+}
+
+/* Units of every game for the current thresholds, grouped by variant. */
+static eg_status batch_plan(eg_batch *b)
+{
+    const int K = b->K;
+    std::vector<UnitDesc> units;
+    std::vector<int> ugame;
+    std::vector<long long> cost;
+    std::vector<size_t> gneed; /* global scratch bytes per unit (0: shared memory) */
+    int smem = 16;
+    for (int g = 0; g < b->num_games; g++) {
+        const size_t before = units.size();
+        EG_TRY(make_units(b->hp[(size_t)g], b->pd[(size_t)g], K, b->d, b->p_host.data() + (size_t)g * K,
+                          b->mg_host.data() + (size_t)g * K, b->p_dev + (size_t)g * K, b->mg_dev + (size_t)g * K,
+                          b->F + b->f_off[(size_t)g], b->smem_budget, b->kg_cap, &units, &gneed, &cost, &smem));
+        for (size_t i = before; i < units.size(); i++) ugame.push_back(g);
+    }
+    std::vector<int> perm;
+    UnitSet S;
+    group_units(units, cost, gneed, &S, &perm);
+    const int nu = (int)S.units.size();
+    size_t gbytes = 0;
+    for (size_t x : S.gneed) gbytes += x;
+    bool reallocated = false;
+    if (nu > b->units_cap || gbytes > b->gscratch_bytes) {
+        reallocated = true;
+        batch_free_units(b);
+        const size_t before = b->bytes;
+        eg_status s = balloc(b, &b->units_dev, (size_t)nu);
+        if (s == EG_OK) s = balloc(b, &b->u_rounds, (size_t)nu);
+        if (s == EG_OK) s = balloc(b, &b->u_status, (size_t)nu);
+        if (s == EG_OK && gbytes) s = balloc(b, (char **)&b->gscratch, gbytes);
+        b->unit_bytes = b->bytes - before;
+        if (s != EG_OK) {
+            batch_free_units(b);
+            return s;
+        }
+        b->units_cap = nu;
+        b->gscratch_bytes = gbytes;
+    }
+    size_t goff = 0;
+    b->unit_game.assign((size_t)nu, 0);
+    for (int j = 0; j < nu; j++) {
+        UnitDesc &u = S.units[(size_t)j];
+        if (S.gneed[(size_t)j]) {
+            u.gscratch = (char *)b->gscratch + goff;
+            goff += S.gneed[(size_t)j];
+        }
+        u.rounds = b->u_rounds + j;
+        u.status = b->u_status + j;
+        b->unit_game[(size_t)j] = ugame[(size_t)perm[(size_t)j]];
+    }
+    /* a captured graph stays valid when the plan is the same (the units read
+     * their thresholds and MG from device memory at run time) */
+    const bool same = !reallocated && b->set.units.size() == S.units.size() &&
+                      memcmp(b->set.off, S.off, sizeof S.off) == 0 && memcmp(b->set.smem, S.smem, sizeof S.smem) == 0 &&
+                      memcmp(b->set.units.data(), S.units.data(), sizeof(UnitDesc) * S.units.size()) == 0;
+    b->set = std::move(S);
+    EG_CUDA(cudaMemcpyAsync(b->units_dev, b->set.units.data(), sizeof(UnitDesc) * (size_t)nu, cudaMemcpyHostToDevice,
+                            b->st));
+    EG_CUDA(cudaStreamSynchronize(b->st));
+    if (!same) batch_drop_graph(b);
     return EG_OK;
 }
 
@@ -620,33 +961,26 @@ extern "C" eg_status eg_batch_set_thresholds(eg_batch *b, const int32_t *p)
 {
     if (!b || !p) return eg_set_error(EG_ERR_INVALID, "NULL argument");
     EG_CUDA(cudaSetDevice(b->device));
-    EG_CUDA(cudaMemcpyAsync(b->thr, p, sizeof(int) * (size_t)b->num_games * b->K, cudaMemcpyHostToDevice, b->st));
-    EG_CUDA(cudaStreamSynchronize(b->st));
+    const int K = b->K;
+    b->p_host.assign(p, p + (size_t)b->num_games * K);
+    b->mg_host.assign((size_t)b->num_games * K, 0);
+    parallel_for(b->num_games, [&](int g) {
+        for (int k = 0; k < K; k++)
+            b->mg_host[(size_t)g * K + k] = threshold_mg(b->hp[(size_t)g], p[(size_t)g * K + k], b->d);
+    });
+    EG_CUDA(cudaMemcpyAsync(b->p_dev, b->p_host.data(), sizeof(int) * b->p_host.size(), cudaMemcpyHostToDevice, b->st));
+    EG_CUDA(cudaMemcpyAsync(b->mg_dev, b->mg_host.data(), sizeof(long long) * b->mg_host.size(), cudaMemcpyHostToDevice,
+                            b->st));
+    EG_TRY(batch_plan(b));
     b->thresholds_set = true;
+    b->solved = false;
     return EG_OK;
 }
 
-static eg_status batch_params(eg_batch *b, BatchParams *p)
+static eg_status batch_enqueue(eg_batch *b, cudaStream_t st, int *grid)
 {
-    memset(p, 0, sizeof *p);
-    p->games = b->desc;
-    p->order = b->order;
-    p->ctrl = b->ctrl;
-    p->num_games = b->num_games;
-    p->words_max = b->words_max;
-    p->max_rounds = b->max_rounds;
-    p->timeout_ns = b->timeout_ms > 0 ? (unsigned long long)(b->timeout_ms * 1e6) : 0ull;
-    return EG_OK;
-}
-
-/* Enqueues one solve (control reset + persistent kernel) on the stream. */
-static eg_status batch_enqueue(eg_batch *b, int block, int *grid_out)
-{
-    BatchParams p;
-    batch_params(b, &p);
-    int sms = 0;
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, b->device);
-    return launch_batch(p, b->KP, block, sms, b->st, grid_out);
+    const unsigned long long tns = b->timeout_ms > 0 ? (unsigned long long)(b->timeout_ms * 1e6) : 0ull;
+    return launch_unit_set(b->launcher, st, b->set, b->units_dev, b->ctrl, b->block, b->sms, b->max_rounds, tns, grid);
 }
 
 extern "C" eg_status eg_batch_solve(eg_batch *b, eg_batch_stats *stats)
@@ -659,18 +993,12 @@ extern "C" eg_status eg_batch_solve(eg_batch *b, eg_batch_stats *stats)
     EG_CUDA(cudaEventRecord(b->ev0, b->st));
     if (b->use_graph) {
         if (!b->graph_exec || b->graph_block != b->block) {
-            if (b->graph_exec) cudaGraphExecDestroy(b->graph_exec);
-            if (b->graph) cudaGraphDestroy(b->graph);
-            b->graph_exec = nullptr;
-            b->graph = nullptr;
+            batch_drop_graph(b);
             /* capture on a side stream so that the timing events stay outside the graph */
             cudaStream_t cs;
             EG_CUDA(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
             EG_CUDA(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
-            cudaStream_t keep = b->st;
-            b->st = cs;
-            eg_status s = batch_enqueue(b, b->block, &grid);
-            b->st = keep;
+            eg_status s = batch_enqueue(b, cs, &grid);
             cudaGraph_t gph = nullptr;
             cudaError_t e = cudaStreamEndCapture(cs, &gph);
             cudaStreamDestroy(cs);
@@ -682,35 +1010,45 @@ extern "C" eg_status eg_batch_solve(eg_batch *b, eg_batch_stats *stats)
             b->graph = gph;
             EG_CUDA(cudaGraphInstantiate(&b->graph_exec, b->graph, 0));
             b->graph_block = b->block;
+            b->graph_grid = grid;
         } else {
             replay = true;
+            grid = b->graph_grid;
         }
         EG_CUDA(cudaGraphLaunch(b->graph_exec, b->st));
     } else {
-        EG_TRY(batch_enqueue(b, b->block, &grid));
+        EG_TRY(batch_enqueue(b, b->st, &grid));
     }
     EG_CUDA(cudaEventRecord(b->ev1, b->st));
-    BatchCtrl c;
-    EG_CUDA(cudaMemcpyAsync(&c, b->ctrl, sizeof c, cudaMemcpyDeviceToHost, b->st));
-    std::vector<long long> rounds((size_t)b->num_games);
-    std::vector<int> status((size_t)b->num_games);
-    EG_CUDA(cudaMemcpyAsync(rounds.data(), b->rounds, sizeof(long long) * rounds.size(), cudaMemcpyDeviceToHost, b->st));
-    EG_CUDA(cudaMemcpyAsync(status.data(), b->status, sizeof(int) * status.size(), cudaMemcpyDeviceToHost, b->st));
+    UnitCtrl cv[kNumVariants];
+    const size_t nu = b->set.units.size();
+    b->last_rounds.assign(nu, 0);
+    b->last_status.assign(nu, 0);
+    EG_CUDA(cudaMemcpyAsync(cv, b->ctrl, sizeof cv, cudaMemcpyDeviceToHost, b->st));
+    EG_CUDA(cudaMemcpyAsync(b->last_rounds.data(), b->u_rounds, sizeof(long long) * nu, cudaMemcpyDeviceToHost, b->st));
+    EG_CUDA(cudaMemcpyAsync(b->last_status.data(), b->u_status, sizeof(int) * nu, cudaMemcpyDeviceToHost, b->st));
     EG_CUDA(cudaStreamSynchronize(b->st));
+    UnitCtrl c;
+    sum_ctrl(cv, &c);
     float ms = 0.f;
     cudaEventElapsedTime(&ms, b->ev0, b->ev1);
     b->solved = true;
-    int failed = 0;
+    std::vector<char> gfail((size_t)b->num_games, 0);
     long long rmax = 0, rsum = 0;
     eg_status first = EG_OK;
-    for (int g = 0; g < b->num_games; g++) {
-        rmax = std::max(rmax, rounds[g]);
-        rsum += rounds[g];
-        if (status[g] != EG_OK) {
-            failed++;
-            if (first == EG_OK) first = (eg_status)status[g];
+    for (size_t i = 0; i < nu; i++) {
+        rmax = std::max(rmax, b->last_rounds[i]);
+        rsum += b->last_rounds[i];
+        if (b->last_status[i] != EG_OK) {
+            gfail[(size_t)b->unit_game[i]] = 1;
+            if (first == EG_OK) first = (eg_status)b->last_status[i];
         }
     }
+    int failed = 0;
+    for (char f : gfail) failed += f;
+    int smem = 0;
+    for (int v = 0; v < kNumVariants; v++)
+        if (b->set.off[v + 1] > b->set.off[v]) smem = std::max(smem, b->set.smem[v]);
     if (stats) {
         memset(stats, 0, sizeof *stats);
         stats->num_games = b->num_games;
@@ -727,6 +1065,8 @@ extern "C" eg_status eg_batch_solve(eg_batch *b, eg_batch_stats *stats)
         stats->grid = grid;
         stats->games_failed = failed;
         stats->graph_replayed = replay ? 1 : 0;
+        stats->num_units = (int32_t)nu;
+        stats->smem_bytes = smem;
     }
     if (first != EG_OK) return eg_set_error(first, "%d game(s) stopped early (status %d)", failed, (int)first);
     return EG_OK;
@@ -737,59 +1077,71 @@ extern "C" eg_status eg_batch_credits(eg_batch *b, int32_t game, int64_t *credit
     if (!b || !credits || game < 0 || game >= b->num_games) return eg_set_error(EG_ERR_INVALID, "bad arguments");
     if (!b->solved) return eg_set_error(EG_ERR_INVALID, "batch not solved");
     EG_CUDA(cudaSetDevice(b->device));
-    const long long base = b->node_off_h[game], n = b->node_off_h[game + 1] - base;
-    std::vector<long long> rows((size_t)(n * b->K));
-    EG_CUDA(cudaMemcpyAsync(rows.data(), b->F + base * b->K, sizeof(long long) * rows.size(), cudaMemcpyDeviceToHost, b->st));
+    const long long cnt = b->f_off[(size_t)game + 1] - b->f_off[(size_t)game];
+    EG_CUDA(cudaMemcpyAsync(credits, b->F + b->f_off[(size_t)game], sizeof(long long) * (size_t)cnt,
+                            cudaMemcpyDeviceToHost, b->st));
     EG_CUDA(cudaStreamSynchronize(b->st));
-    for (long long v = 0; v < n; v++)
-        for (int k = 0; k < b->K; k++) credits[(size_t)k * n + v] = rows[(size_t)(v * b->K + k)];
     return EG_OK;
 }
 
 extern "C" eg_status eg_batch_game_result(eg_batch *b, int32_t game, int64_t *rounds, int32_t *status)
 {
     if (!b || game < 0 || game >= b->num_games) return eg_set_error(EG_ERR_INVALID, "bad arguments");
-    EG_CUDA(cudaSetDevice(b->device));
+    if (!b->solved) return eg_set_error(EG_ERR_INVALID, "batch not solved");
     long long r = 0;
-    int s = 0;
-    EG_CUDA(cudaMemcpyAsync(&r, b->rounds + game, sizeof r, cudaMemcpyDeviceToHost, b->st));
-    EG_CUDA(cudaMemcpyAsync(&s, b->status + game, sizeof s, cudaMemcpyDeviceToHost, b->st));
-    EG_CUDA(cudaStreamSynchronize(b->st));
+    int s = EG_OK;
+    for (size_t i = 0; i < b->set.units.size(); i++) {
+        if (b->unit_game[i] != game) continue;
+        r = std::max(r, b->last_rounds[i]);
+        if (s == EG_OK && b->last_status[i] != EG_OK) s = b->last_status[i];
+    }
     if (rounds) *rounds = r;
     if (status) *status = s;
     return EG_OK;
 }
 
-/* Autotuner: each candidate CTA size solves the batch under a round cap
- * (enough rounds to reach steady state, few enough to be quick); the one
- * with the most edge relaxations per second is kept. */
+/* Autotuner: every candidate (CTA size, largest threshold group) plans the
+ * batch and solves it under a sweep cap (enough sweeps to reach the steady
+ * state, few enough to be quick); the candidate with the most edge
+ * relaxations per second is kept. */
 extern "C" eg_status eg_batch_tune(eg_batch *b, int32_t *block_out)
 {
     if (!b) return eg_set_error(EG_ERR_INVALID, "batch is NULL");
     if (!b->thresholds_set) return eg_set_error(EG_ERR_INVALID, "thresholds not set");
-    const int cands[] = {256, 512, 1024};
+    const int blocks[] = {512, 1024};
+    const int groups[] = {8, 4, 2, 1};
     const long long keep_cap = b->max_rounds;
     const bool keep_graph = b->use_graph;
+    const int keep_kg = b->kg_cap;
     b->use_graph = false;
-    b->max_rounds = 64;
+    b->max_rounds = 48;
     double best = -1.0;
-    int best_block = b->block;
-    for (int c : cands) {
-        b->block = c;
-        eg_batch_stats st;
-        eg_status s = eg_batch_solve(b, &st);
-        if (s != EG_OK && s != EG_ERR_LOOPCAP) continue;
-        const double rate = st.solve_ms > 0 ? (double)st.edges / st.solve_ms : 0.0;
-        if (rate > best) {
-            best = rate;
-            best_block = c;
+    int best_block = b->block, best_kg = keep_kg;
+    for (int kg : groups) {
+        if (kg > keep_kg) continue;
+        b->kg_cap = kg;
+        eg_status ps = batch_plan(b);
+        if (ps != EG_OK) continue;
+        for (int c : blocks) {
+            b->block = c;
+            eg_batch_stats st;
+            eg_status s = eg_batch_solve(b, &st);
+            if (s != EG_OK && s != EG_ERR_LOOPCAP) continue;
+            const double rate = st.solve_ms > 0 ? (double)st.edges / st.solve_ms : 0.0;
+            if (rate > best) {
+                best = rate;
+                best_block = c;
+                best_kg = kg;
+            }
         }
     }
     b->block = best_block;
+    b->kg_cap = best_kg;
     b->max_rounds = keep_cap;
     b->use_graph = keep_graph;
     b->solved = false;
+    EG_TRY(batch_plan(b));
     if (block_out) *block_out = best_block;
-    if (best < 0) return eg_set_error(EG_ERR_CUDA, "no candidate CTA size ran");
+    if (best < 0) return eg_set_error(EG_ERR_CUDA, "no candidate ran");
     return EG_OK;
 }

@@ -1,76 +1,178 @@
 /*
- * eg_batch.cuh -- the per-game descriptor and launch interface of the
- * batched (CTA-per-game, K thresholds on K lanes) solver, shared by the
- * batch API and the serving loop.
+ * eg_batch.cuh -- the packed game layout, the work units and the launch
+ * interface of the batched solver (many games x K thresholds per launch),
+ * shared by the batch API (eg_batch.cu) and the serving loop (eg_serve.cu).
+ *
+ * Packed layout of one game.  Vertices are renumbered by (owner, out-degree):
+ * player-0 vertices first, each owner class padded with dummy vertices to a
+ * multiple of 32, so that slice s = new ids [32 s, 32 s + 32) belongs to one
+ * owner.  Each slice stores its out-edges column-major (an ELL block of
+ * width = the slice's largest out-degree): slot (j, lane) holds edge j of
+ * vertex 32 s + lane, so a warp reads one column as one 128-byte line.
+ * Missing edges are pads that cannot change the vertex's min (player 0:
+ * an edge to the sentinel row TOPROW, credit TOP, weight -wpad) or max
+ * (player 1: an edge to the sentinel row LOWROW, credit far below 0, weight
+ * +wpad), where wpad = max |w| + 1.  A slot is 4 bytes {u16 successor,
+ * i16 weight} when the ids and weights fit, else 8 bytes {i32, i32}.
+ *
+ * The weight of threshold p at scale d is w * d - p (a mean-payoff query
+ * "mean payoff >= p/d" as an energy game).  The slots keep w; the kernel
+ * forms w * d and adds p once per vertex (OMINUS's clamp is monotone, so
+ * min/max over the edges commute with it).
  */
 #ifndef EG_BATCH_CUH
 #define EG_BATCH_CUH
 
 #include "eg_prep.cuh"
 
+#include <vector>
+
 namespace eg {
 
-/* One game to solve at K thresholds.  Vertex ids stored in E and CS are
- * base + local id; P, CP, owner, minw, maxw and F are indexed by the local
- * id (F[local * K + k]). */
-struct GameDesc {
-    const int *P;              /* n + 1 offsets into E                      */
-    const int2 *E;             /* {successor id, weight}                    */
-    const int *CP;             /* n + 1 offsets into CS                     */
-    const int *CS;             /* predecessor ids                           */
-    const unsigned char *owner;
-    const int *minw, *maxw;    /* min / max out-weight per vertex           */
-    const int *thr;            /* K thresholds p_k                          */
-    long long *F;              /* credits, n * K                            */
-    long long *rounds;         /* out: rounds run                           */
-    int *status;               /* out: eg_status                            */
-    long long base;
-    int n, K, d, pad;
-};
-
-struct BatchCtrl {
-    int next_game;
-    int pad;
-    unsigned long long lifts, edges, num_top;
-    unsigned long long t_start;
-};
-
-struct BatchParams {
-    const GameDesc *games;     /* device array                              */
-    const int *order;          /* queue order (largest first), or NULL      */
-    BatchCtrl *ctrl;
-    int num_games;
-    int words_max;             /* shared bitmap words per buffer            */
-    long long max_rounds;
-    unsigned long long timeout_ns;
-};
-
-/* One game uploaded in the batched kernel's layout (local ids, base 0). */
-struct GameLayout {
-    int *P, *CP, *CS, *minw, *maxw;
-    int2 *E;
-    unsigned char *owner;
-    int n;
-    long long m;
-    size_t bytes;
-};
-/* Device bytes a game's layout takes (plus the sort's temporaries while it
- * is built). */
-size_t layout_bytes(int n, long long m);
-size_t layout_build_bytes(int n, long long m);
-/* Uploads the game and builds its CSC on the device (synchronous on st). */
-eg_status layout_upload(const eg_game &g, cudaStream_t st, GameLayout *out);
-void layout_free(GameLayout *l, cudaStream_t st);
-/* A descriptor of a laid-out game for one query. */
-GameDesc layout_desc(const GameLayout &l, const int *thr, long long *F, long long *rounds, int *status, int K, int d);
-
-/* Largest game (vertices) the shared-memory frontier of the batched kernel holds. */
+/* Largest game the batched paths take (larger games go to the grid solver). */
 constexpr int kBatchMaxGameNodes = 1 << 19;
 
-/* Resets ctrl and launches the batched kernel (lanes = KP, a power of two
- * >= every game's K) with `block` threads per CTA on `st`; *grid gets the
- * number of CTAs. */
-eg_status launch_batch(const BatchParams &p, int KP, int block, int num_sms, cudaStream_t st, int *grid);
+/* Host image of one packed game. */
+struct HostPacked {
+    int n = 0, n0 = 0, n1 = 0;   /* vertices, of player 0, of player 1         */
+    int ns = 0, s0 = 0;          /* slices; first slice of player 1            */
+    long long m = 0;             /* real edges                                 */
+    long long slots = 0;         /* slots incl. pads (32 per column)           */
+    int wide = 0;                /* 8-byte slots                               */
+    int wpad = 1;                /* max |w| + 1                                */
+    int maxdeg = 0;
+    std::vector<uint32_t> e32;   /* narrow slots                               */
+    std::vector<int2> e64;       /* wide slots                                 */
+    std::vector<int> slice_off;  /* ns + 1 slot offsets                        */
+    std::vector<int> orig;       /* 32 ns: new id -> original id, -1 dummy     */
+    std::vector<int> minw;       /* per original vertex: min out-weight        */
+    int rows() const { return 32 * ns + 2; }
+};
+
+/* Builds the packed layout of g (owners from g.owner or the n0 split). */
+eg_status pack_game(const eg_game &g, HostPacked *out);
+
+/* Device image of one packed game (E, slice_off and orig in one block). */
+struct PackedDev {
+    void *E = nullptr;
+    int *slice_off = nullptr;
+    int *orig = nullptr;
+    void *block = nullptr;       /* the one allocation holding all three       */
+    size_t bytes = 0;
+};
+size_t packed_dev_bytes(const HostPacked &h);
+/* Uploads into `block` (caller-allocated, packed_dev_bytes(h) bytes). */
+eg_status packed_upload(const HostPacked &h, void *block, cudaStream_t st, PackedDev *out);
+
+/* MG of threshold p at scale d: sum_v max(0, p - d * minw(v)). */
+long long threshold_mg(const HostPacked &h, int p, int d);
+
+/* Unit variant bits. */
+enum : int {
+    kUnitKgMask = 3,       /* log2 of the thresholds in the unit (1, 2, 4, 8) */
+    kUnitCredit64 = 4,     /* 64-bit credits                                    */
+    kUnitWide = 8,         /* 8-byte slots                                      */
+    kUnitGlobal = 16       /* credits in global scratch (too large for shared)  */
+};
+
+/* One work unit: a game at a group of kg = 2^(variant & 3) consecutive
+ * thresholds k0 .. k0 + kg - 1, solved by one CTA. */
+struct UnitDesc {
+    const void *E;
+    const int *slice_off;
+    const int *orig;
+    const int *p;              /* thresholds of the game (index k)            */
+    const long long *mg;       /* MG per threshold (index k)                  */
+    long long *F;              /* credits out: F[k * n + v], TOP = INT64_MAX  */
+    void *gscratch;            /* rows * kg credits when kUnitGlobal          */
+    long long *rounds;         /* out: sweeps run                             */
+    int *status;               /* out: eg_status                              */
+    long long m;
+    int n, n0, n1, ns, s0;
+    int d, k0, variant;
+    int pad;
+};
+
+struct UnitCtrl {
+    int next;
+    int pad;
+    unsigned long long lifts, edges, num_top;
+    unsigned long long t_begin, t_end; /* device clock (ns): first CTA start, last CTA end */
+};
+
+struct UnitParams {
+    const UnitDesc *units;
+    UnitCtrl *ctrl;
+    int num_units;
+    int pad;
+    long long max_rounds;          /* per unit; < 0: none                        */
+    unsigned long long timeout_ns; /* per launch, from each CTA's start; 0: none */
+};
+
+/* Choice of credit width and group size for a game. */
+struct UnitPlan {
+    int credit64;   /* 1: 64-bit credits needed                               */
+    int kg_max;     /* largest group that fits shared memory (0: global)      */
+};
+/* True when 32-bit credits are exact for every threshold of the list:
+ * MG + wpad * d + |p| < 2^30 (the sentinel TOP is 2^30). */
+bool credits32_ok(const HostPacked &h, const int *p, int K, int d, const long long *mg);
+UnitPlan plan_game(const HostPacked &h, bool credit64, int smem_budget, int kg_cap);
+/* Splits K thresholds into groups of 8/4/2/1 of at most kg_max (kg_max 0:
+ * groups of one, credits in global scratch); appends (k0, log2 kg). */
+void split_thresholds(int K, int kg_max, std::vector<std::pair<int, int>> *groups);
+
+/* Appends the units of one game at K thresholds: p / mg are the host
+ * values, p_dev / mg_dev / F_dev the device arrays the units read and
+ * write (F_dev[k * n + v]).  Per unit it also appends the global scratch
+ * bytes it needs (0: shared memory) and a cost estimate; *smem grows to
+ * the shared memory the units need.  Fails with EG_ERR_OVERFLOW when a
+ * threshold's MG does not fit 61 bits. */
+eg_status make_units(const HostPacked &h, const PackedDev &pd, int K, int d, const int *p, const long long *mg,
+                     const int *p_dev, const long long *mg_dev, long long *F_dev, int smem_budget, int kg_cap,
+                     std::vector<UnitDesc> *units, std::vector<size_t> *gneed, std::vector<long long> *cost,
+                     int *smem);
+
+/* Unit variants are indexes 0 .. kNumVariants - 1 (the bits above). */
+constexpr int kNumVariants = 32;
+
+/* Units grouped by variant, heaviest first within a variant:
+ * units[off[v] .. off[v + 1]) have variant v. */
+struct UnitSet {
+    std::vector<UnitDesc> units;
+    std::vector<size_t> gneed;        /* global scratch bytes per unit          */
+    int off[kNumVariants + 1];
+    int smem[kNumVariants];           /* dynamic shared memory per variant      */
+    long long top_cost[kNumVariants]; /* heaviest unit of the variant           */
+};
+/* Groups units (with their costs and scratch needs); perm[i] = index in
+ * `units` of the i-th grouped unit. */
+void group_units(const std::vector<UnitDesc> &units, const std::vector<long long> &cost,
+                 const std::vector<size_t> &gneed, UnitSet *out, std::vector<int> *perm);
+
+/* Shared memory the kernels can be launched with (the opt-in maximum). */
+int unit_smem_budget(int device);
+/* Opts every unit kernel in to that much dynamic shared memory (per device). */
+eg_status unit_kernel_setup(int device);
+
+/* Side streams on which the variants of a unit set run concurrently: the
+ * launch forks from a main stream and joins back into it, so it can be
+ * captured into a CUDA graph. */
+struct UnitLauncher {
+    cudaStream_t aux[kNumVariants] = {};
+    cudaEvent_t join[kNumVariants] = {};
+    cudaEvent_t fork = nullptr;
+    eg_status init();
+    void destroy();
+};
+/* Launches one persistent kernel per variant present in S (the variant
+ * holding the heaviest unit first), each taking its units from its own
+ * queue; ctrl_dev holds kNumVariants counters, reset on `main` first. */
+eg_status launch_unit_set(UnitLauncher &L, cudaStream_t main, const UnitSet &S, const UnitDesc *units_dev,
+                          UnitCtrl *ctrl_dev, int block, int num_sms, long long max_rounds,
+                          unsigned long long timeout_ns, int *grid_total);
+/* Totals of the per-variant counters. */
+void sum_ctrl(const UnitCtrl *c, UnitCtrl *out);
 
 }  // namespace eg
 

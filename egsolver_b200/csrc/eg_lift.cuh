@@ -8,6 +8,10 @@
 
 namespace eg {
 
+/* Most sweeps of the edge stream per grid barrier in dense rounds (one bank
+ * of cut-vertex accumulators each). */
+constexpr int kMaxDenseSweeps = 4;
+
 /* Lane-group sizes of the lifting variants; EG_GROUP_CTA lifts one vertex
  * with the whole CTA. */
 enum { EG_GROUP_CTA = 0, EG_GROUP_LIGHT = 64 };
@@ -61,7 +65,7 @@ struct LiftParams {
     int wbits, wbias;          /* packed edge: (succ << wbits) | (w + wbias)       */
     int fast32;                /* 32-bit credits whose differences fit 32 bits     */
     int dense_depth;           /* chunks in flight per warp: 1 (3 CTAs per SM) or 2 */
-    int dense_sweeps;          /* sweeps of every slice per grid barrier: 1 or 2    */
+    int dense_sweeps;          /* sweeps of every slice per grid barrier: 1 .. 4    */
 };
 
 /* Round kinds, as Ctrl::next_mode holds them between rounds and launches. */

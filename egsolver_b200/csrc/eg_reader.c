@@ -22,6 +22,7 @@
 #include <stdio.h>
 #include <stdlib.h>
 #include <string.h>
+#include <sys/stat.h>
 #include <zlib.h>
 
 enum { T_EOF = 0, T_INT, T_FLOAT, T_STRING, T_ARENA, T_MAX, T_MIN, T_SEMI, T_COL, T_COMMA, T_MINUS, T_ERR };
@@ -325,4 +326,154 @@ eg_status eg_read_game_file(const char *path, const eg_read_opts *ropts, eg_owne
     st = eg_read_game_buffer(buf, len, ropts, out);
     free(buf);
     return st;
+}
+
+/* ------------------------------------------------------------------ */
+/* Binary CSR cache                                                     */
+/* ------------------------------------------------------------------ */
+
+/* A game as read (owner-sorted CSR, external names, reader options) in a
+ * flat little-endian file, so that a large game parsed once from text is
+ * loaded again at memory speed:
+ *
+ *   header (64 bytes): magic "EGCSR\1\0\0", n, n0 (int32), m (int64),
+ *       max |w| (int32), weight mode, rnd lo, rnd hi (int32), rnd seed
+ *       (uint64), FNV-1a 64 checksum of the arrays (uint64), 8 bytes zero
+ *   row_ptr int64[n + 1] | succ int32[m] | weight int32[m] | ext_id int32[n]
+ */
+typedef struct {
+    char magic[8];
+    int32_t n, n0;
+    int64_t m;
+    int32_t max_abs_weight, weight_mode, rnd_lo, rnd_hi;
+    uint64_t rnd_seed, checksum, zero;
+} egb_header;
+
+static const char EGB_MAGIC[8] = {'E', 'G', 'C', 'S', 'R', 1, 0, 0};
+
+static uint64_t fnv1a(uint64_t h, const void *p, size_t len)
+{
+    const unsigned char *c = (const unsigned char *)p;
+    for (size_t i = 0; i < len; i++) {
+        h ^= c[i];
+        h *= 0x100000001b3ULL;
+    }
+    return h;
+}
+
+static uint64_t egb_checksum(const eg_owned_game *g)
+{
+    const int32_t n = g->game.num_nodes;
+    const int64_t m = g->game.num_edges;
+    uint64_t h = 0xcbf29ce484222325ULL;
+    h = fnv1a(h, g->row_ptr, sizeof(int64_t) * ((size_t)n + 1));
+    h = fnv1a(h, g->succ, sizeof(int32_t) * (size_t)m);
+    h = fnv1a(h, g->weight, sizeof(int32_t) * (size_t)m);
+    return fnv1a(h, g->ext_id, sizeof(int32_t) * (size_t)n);
+}
+
+static void egb_opts(const eg_read_opts *ro, egb_header *h)
+{
+    h->weight_mode = ro ? ro->weight_mode : 0;
+    h->rnd_lo = ro && ro->weight_mode == 3 ? ro->rnd_lo : 0;
+    h->rnd_hi = ro && ro->weight_mode == 3 ? ro->rnd_hi : 0;
+    h->rnd_seed = ro && ro->weight_mode == 3 ? ro->rnd_seed : 0;
+}
+
+eg_status eg_write_game_binary(const char *path, const eg_owned_game *g, const eg_read_opts *ropts)
+{
+    if (!path || !g) return eg_set_error(EG_ERR_INVALID, "NULL argument");
+    egb_header h;
+    memset(&h, 0, sizeof h);
+    memcpy(h.magic, EGB_MAGIC, 8);
+    h.n = g->game.num_nodes;
+    h.n0 = g->game.num_nodes0;
+    h.m = g->game.num_edges;
+    h.max_abs_weight = g->max_abs_weight;
+    egb_opts(ropts, &h);
+    h.checksum = egb_checksum(g);
+    FILE *f = fopen(path, "wb");
+    if (!f) return eg_set_error(EG_ERR_IO, "cannot create %s: %s", path, strerror(errno));
+    int ok = fwrite(&h, sizeof h, 1, f) == 1;
+    ok = ok && fwrite(g->row_ptr, sizeof(int64_t), (size_t)h.n + 1, f) == (size_t)h.n + 1;
+    ok = ok && fwrite(g->succ, sizeof(int32_t), (size_t)h.m, f) == (size_t)h.m;
+    ok = ok && fwrite(g->weight, sizeof(int32_t), (size_t)h.m, f) == (size_t)h.m;
+    ok = ok && fwrite(g->ext_id, sizeof(int32_t), (size_t)h.n, f) == (size_t)h.n;
+    ok = (fclose(f) == 0) && ok;
+    if (!ok) return eg_set_error(EG_ERR_IO, "error writing %s", path);
+    return EG_OK;
+}
+
+eg_status eg_read_game_binary(const char *path, const eg_read_opts *ropts, eg_owned_game **out)
+{
+    if (!path || !out) return eg_set_error(EG_ERR_INVALID, "NULL argument");
+    FILE *f = fopen(path, "rb");
+    if (!f) return eg_set_error(EG_ERR_IO, "cannot open %s: %s", path, strerror(errno));
+    egb_header h;
+    if (fread(&h, sizeof h, 1, f) != 1 || memcmp(h.magic, EGB_MAGIC, 8) != 0 || h.n <= 0 || h.m < 0 ||
+        h.n0 < 0 || h.n0 > h.n || h.m > (int64_t)INT32_MAX) {
+        fclose(f);
+        return eg_set_error(EG_ERR_IO, "%s is not a binary game file", path);
+    }
+    egb_header want;
+    memset(&want, 0, sizeof want);
+    egb_opts(ropts, &want);
+    if (ropts && (want.weight_mode != h.weight_mode || want.rnd_lo != h.rnd_lo || want.rnd_hi != h.rnd_hi ||
+                  want.rnd_seed != h.rnd_seed)) {
+        fclose(f);
+        return eg_set_error(EG_ERR_IO, "%s was written with other reader options", path);
+    }
+    eg_owned_game *g = eg_owned_game_alloc(h.n, h.m);
+    if (!g) {
+        fclose(f);
+        return eg_set_error(EG_ERR_OOM, "host allocation failed");
+    }
+    int ok = fread(g->row_ptr, sizeof(int64_t), (size_t)h.n + 1, f) == (size_t)h.n + 1;
+    ok = ok && fread(g->succ, sizeof(int32_t), (size_t)h.m, f) == (size_t)h.m;
+    ok = ok && fread(g->weight, sizeof(int32_t), (size_t)h.m, f) == (size_t)h.m;
+    ok = ok && fread(g->ext_id, sizeof(int32_t), (size_t)h.n, f) == (size_t)h.n;
+    fclose(f);
+    g->game.num_nodes0 = h.n0;
+    g->max_abs_weight = h.max_abs_weight;
+    if (!ok || egb_checksum(g) != h.checksum) {
+        eg_owned_game_free(g);
+        return eg_set_error(EG_ERR_IO, "%s is truncated or corrupt (checksum)", path);
+    }
+    eg_status st = eg_validate(&g->game);
+    if (st != EG_OK) {
+        eg_owned_game_free(g);
+        return st;
+    }
+    *out = g;
+    return EG_OK;
+}
+
+eg_status eg_read_game_file_cached(const char *path, const eg_read_opts *ropts, const char *cache_path,
+                                   eg_owned_game **out)
+{
+    if (!path || !cache_path || !out) return eg_set_error(EG_ERR_INVALID, "NULL argument");
+    struct stat sp, sc;
+    if (stat(path, &sp) == 0 && stat(cache_path, &sc) == 0 && sc.st_mtime >= sp.st_mtime) {
+        eg_owned_game *g = NULL;
+        if (eg_read_game_binary(cache_path, ropts, &g) == EG_OK) {
+            *out = g;
+            return EG_OK;
+        }
+    }
+    eg_status st = eg_read_game_file(path, ropts, out);
+    if (st != EG_OK) return st;
+    /* best effort: a cache that cannot be written leaves the result alone */
+    size_t len = strlen(cache_path);
+    char *tmp = (char *)malloc(len + 8);
+    if (tmp) {
+        memcpy(tmp, cache_path, len);
+        memcpy(tmp + len, ".tmp", 5);
+        if (eg_write_game_binary(tmp, *out, ropts) == EG_OK) {
+            if (rename(tmp, cache_path) != 0) remove(tmp);
+        } else {
+            remove(tmp);
+        }
+        free(tmp);
+    }
+    return EG_OK;
 }

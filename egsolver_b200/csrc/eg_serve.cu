@@ -10,21 +10,27 @@
  *   2. admission, in submission order: a query is admitted when fewer than
  *      max_inflight queries are admitted and the free device memory (from
  *      cudaMemGetInfo) minus hbm_reserve_bytes covers its credits and, if
- *      its game is not resident yet, the game's CSR/CSC; idle resident games
- *      are evicted oldest-first when memory is short.  A game stays resident
- *      across all its queries until it is evicted or removed;
+ *      its game is not resident yet, the game's packed layout; idle resident
+ *      games are evicted oldest-first when memory is short.  A game stays
+ *      resident across all its queries until it is evicted or removed;
  *   3. launch: every admitted query not yet launched goes into one
- *      micro-batch, i.e. one launch of the batched kernel (one CTA per query,
- *      thresholds on lanes), on the next of `streams` streams.  Earlier
- *      micro-batches keep running, so the work of queries that arrived at
- *      different times overlaps on the device.
+ *      micro-batch, i.e. one launch of the unit kernel (eg_batch.cu: one CTA
+ *      per game x threshold group, credits in shared memory), on the next of
+ *      `streams` streams.  Earlier micro-batches keep running; as their CTAs
+ *      run out of units and exit, the new launch's CTAs take the freed SMs,
+ *      so the work of queries that arrived at different times overlaps on
+ *      the device.  Each launch records its first CTA start and last CTA end
+ *      on the device clock (eg_serve_trace).
  *
- * Games above the batched kernel's size limit (2^19 vertices) are solved by
- * a second thread, one threshold at a time, on the persistent grid solver
- * capped at `large_ctas` CTAs so that micro-batches keep SMs to run on.
+ * Routing: games above the batched layout's limit (2^19 vertices), and games
+ * whose credits do not fit one CTA's shared memory while the queue is
+ * shallow, are solved by a second thread one threshold at a time on the
+ * persistent grid solver, capped at `large_ctas` CTAs so that micro-batches
+ * keep SMs to run on.  With a deep queue such games run as units with their
+ * credits in global memory, for throughput.
  *
- * Every result equals the solve of the same game and threshold alone: the
- * kernel's work per query depends only on that query's data.
+ * Every result equals the solve of the same game and threshold alone: a
+ * unit's work depends only on its own game and thresholds.
  */
 #include "eg_batch.cuh"
 #include "../../include/egsolver_b200_serve.h"
@@ -56,10 +62,12 @@ struct ServedGame {
     std::vector<int32_t> succ, w;
     std::vector<uint8_t> own;
     bool has_owner = false;
-    bool large = false;
+    bool large = false;          /* above the batched layout's limit         */
+    bool fits_smem = true;       /* one threshold's credits fit shared memory */
     bool resident = false;
     bool removed = false;
-    GameLayout L{};
+    HostPacked hp;               /* packed layout (host image)               */
+    PackedDev pd;                /* its device copy while resident           */
     int active = 0; /* admitted queries still running */
     uint64_t last_use = 0;
     eg_game view() const
@@ -85,21 +93,30 @@ struct Query {
     clk::time_point t_submit, t_done;
     long long rounds = 0;
     std::vector<int64_t> result; /* threshold-major */
-    /* device buffers while admitted: credits n*K, thresholds, rounds, status */
+    std::vector<long long> mg;   /* MG per threshold                         */
+    /* device buffers while admitted: credits n*K (threshold-major),
+     * thresholds, MG, per-unit rounds and status, global credit scratch */
     long long *dF = nullptr;
     int *dthr = nullptr;
+    long long *dmg = nullptr;
     long long *drounds = nullptr;
     int *dstatus = nullptr;
+    void *dscratch = nullptr;
     size_t dbytes = 0;
+    std::vector<UnitDesc> units; /* planned at admission                     */
+    std::vector<long long> cost;
+    int smem = 16;
     cudaEvent_t ready = nullptr; /* buffers allocated and thresholds copied */
 };
 
 struct Launch {
     int stream;
+    int64_t number = 0;
+    int units = 0;
     cudaEvent_t ev = nullptr;
     std::vector<int64_t> qids;
-    GameDesc *ddesc = nullptr;
-    BatchCtrl *dctrl = nullptr;
+    UnitDesc *dunits = nullptr;
+    UnitCtrl *dctrl = nullptr;
 };
 
 }  // namespace
@@ -117,11 +134,15 @@ struct eg_server {
     std::vector<int64_t> ready;
     std::vector<Launch> inflight;
     std::vector<cudaStream_t> streams;
+    std::vector<UnitLauncher> launchers; /* side streams of each micro-batch stream */
     cudaStream_t upload_stream = nullptr;
     int next_stream = 0;
     int admitted_now = 0;
     uint64_t tick = 0;
     int sms = 148;
+    int smem_budget = 0;
+    std::vector<eg_serve_span> spans;   /* device-clock span of every micro-batch */
+    unsigned long long clock0 = 0;      /* device clock of the first micro-batch  */
     /* statistics */
     int64_t submitted = 0, admitted = 0, completed = 0, failed = 0, uploads = 0, evictions = 0;
     int64_t micro_batches = 0, threshold_solves = 0;
@@ -132,7 +153,11 @@ struct eg_server {
 
 namespace {
 
-size_t query_bytes(const ServedGame &g, int K) { return sizeof(long long) * (size_t)g.n * K + 64 * sizeof(int) + 256; }
+/* credits | thresholds | MG | per-unit rounds | per-unit status | scratch */
+size_t query_bytes(const ServedGame &g, int K, size_t scratch)
+{
+    return sizeof(long long) * (size_t)g.n * K + 4 * 64 * sizeof(long long) + 1024 + scratch;
+}
 
 void free_query_device(Query &q, cudaStream_t st)
 {
@@ -141,8 +166,19 @@ void free_query_device(Query &q, cudaStream_t st)
     q.ready = nullptr;
     q.dF = nullptr;
     q.dthr = nullptr;
+    q.dmg = nullptr;
     q.drounds = nullptr;
     q.dstatus = nullptr;
+    q.dscratch = nullptr;
+}
+
+void drop_resident(eg_server *s, ServedGame &g)
+{
+    s->device_bytes -= (int64_t)g.pd.bytes;
+    if (g.pd.block) cudaFreeAsync(g.pd.block, s->upload_stream);
+    cudaStreamSynchronize(s->upload_stream);
+    g.pd = PackedDev();
+    g.resident = false;
 }
 
 /* Frees resident games nobody uses, oldest first, until `need` bytes fit. */
@@ -162,10 +198,7 @@ bool make_room(eg_server *s, size_t need)
             if (g.resident && g.active == 0 && (!victim || g.last_use < victim->last_use)) victim = &g;
         }
         if (!victim) return false;
-        s->device_bytes -= (int64_t)victim->L.bytes;
-        layout_free(&victim->L, s->upload_stream);
-        cudaStreamSynchronize(s->upload_stream);
-        victim->resident = false;
+        drop_resident(s, *victim);
         s->evictions++;
     }
 }
@@ -198,25 +231,41 @@ bool reap(eg_server *s)
         }
         any = true;
         const clk::time_point now = clk::now();
+        UnitCtrl c, cv[kNumVariants];
+        memset(&c, 0, sizeof c);
+        if (e == cudaSuccess && cudaMemcpy(cv, l.dctrl, sizeof cv, cudaMemcpyDeviceToHost) == cudaSuccess) {
+            sum_ctrl(cv, &c);
+            if (!s->clock0) s->clock0 = c.t_begin;
+            eg_serve_span sp;
+            memset(&sp, 0, sizeof sp);
+            sp.batch = l.number;
+            sp.queries = (int32_t)l.qids.size();
+            sp.units = l.units;
+            sp.begin_ms = ((double)c.t_begin - (double)s->clock0) * 1e-6;
+            sp.end_ms = ((double)c.t_end - (double)s->clock0) * 1e-6;
+            s->spans.push_back(sp);
+        }
         for (int64_t qid : l.qids) {
             Query &q = *s->queries[qid];
             ServedGame &g = *s->games[q.game];
             eg_status st = e == cudaSuccess ? EG_OK : EG_ERR_CUDA;
             if (st == EG_OK) {
-                std::vector<long long> rows((size_t)g.n * q.K);
-                int dst = 0;
-                long long r = 0;
-                cudaError_t c = cudaMemcpy(rows.data(), q.dF, sizeof(long long) * rows.size(), cudaMemcpyDeviceToHost);
-                if (c == cudaSuccess) c = cudaMemcpy(&dst, q.dstatus, sizeof dst, cudaMemcpyDeviceToHost);
-                if (c == cudaSuccess) c = cudaMemcpy(&r, q.drounds, sizeof r, cudaMemcpyDeviceToHost);
-                if (c != cudaSuccess) {
+                const size_t nu = q.units.size();
+                std::vector<long long> rr(nu);
+                std::vector<int> ss(nu);
+                q.result.assign((size_t)g.n * q.K, 0);
+                cudaError_t cp = cudaMemcpy(q.result.data(), q.dF, sizeof(long long) * q.result.size(),
+                                            cudaMemcpyDeviceToHost);
+                if (cp == cudaSuccess) cp = cudaMemcpy(ss.data(), q.dstatus, sizeof(int) * nu, cudaMemcpyDeviceToHost);
+                if (cp == cudaSuccess) cp = cudaMemcpy(rr.data(), q.drounds, sizeof(long long) * nu, cudaMemcpyDeviceToHost);
+                if (cp != cudaSuccess) {
                     st = EG_ERR_CUDA;
                 } else {
-                    q.rounds = r;
-                    st = (eg_status)dst;
-                    q.result.assign((size_t)g.n * q.K, 0);
-                    for (int v = 0; v < g.n; v++)
-                        for (int k = 0; k < q.K; k++) q.result[(size_t)k * g.n + v] = rows[(size_t)v * q.K + k];
+                    q.rounds = 0;
+                    for (size_t u = 0; u < nu; u++) {
+                        q.rounds = std::max(q.rounds, rr[u]);
+                        if (st == EG_OK && ss[u] != EG_OK) st = (eg_status)ss[u];
+                    }
                 }
             }
             s->device_bytes -= (int64_t)q.dbytes;
@@ -226,7 +275,7 @@ bool reap(eg_server *s)
             finish_query(s, q, st, now);
         }
         cudaEventDestroy(l.ev);
-        cudaFreeAsync(l.ddesc, s->streams[l.stream]);
+        cudaFreeAsync(l.dunits, s->streams[l.stream]);
         cudaFreeAsync(l.dctrl, s->streams[l.stream]);
         s->inflight.erase(s->inflight.begin() + (long)i);
     }
@@ -242,15 +291,37 @@ bool admit(eg_server *s, std::unique_lock<std::mutex> &lk)
         const int64_t qid = s->pending.front();
         Query &q = *s->queries[qid];
         ServedGame &g = *s->games[q.game];
-        if (g.large) {
+        /* routing: the grid solver for games the batched layout cannot hold,
+         * and for games whose credits miss shared memory while the queue is
+         * shallow (lower latency); units otherwise */
+        if (g.large || (!g.fits_smem && s->pending.size() + s->ready.size() <= 2)) {
             s->pending.pop_front();
             s->large_pending.push_back(qid);
             s->cv_work.notify_all();
             any = true;
             continue;
         }
-        size_t need = query_bytes(g, q.K);
-        if (!g.resident) need += layout_bytes(g.n, g.m) + layout_build_bytes(g.n, g.m);
+        /* plan the query's units (device pointers are filled in below) */
+        q.mg.assign((size_t)q.K, 0);
+        for (int k = 0; k < q.K; k++) q.mg[(size_t)k] = threshold_mg(g.hp, q.p[(size_t)k], q.d);
+        std::vector<UnitDesc> units;
+        std::vector<size_t> gneed;
+        std::vector<long long> cost;
+        int smem = 16;
+        eg_status ps = make_units(g.hp, PackedDev(), q.K, q.d, q.p.data(), q.mg.data(), nullptr, nullptr, nullptr,
+                                  s->smem_budget, 8, &units, &gneed, &cost, &smem);
+        if (ps != EG_OK) {
+            s->pending.pop_front();
+            finish_query(s, q, ps, clk::now());
+            s->cv_done.notify_all();
+            any = true;
+            continue;
+        }
+        size_t scratch = 0;
+        for (size_t x : gneed) scratch += x;
+        const size_t qbytes = query_bytes(g, q.K, scratch) + units.size() * 16;
+        size_t need = qbytes;
+        if (!g.resident) need += packed_dev_bytes(g.hp);
         if (!make_room(s, need)) {
             if (s->admitted_now == 0 && s->inflight.empty()) { /* can never fit */
                 s->pending.pop_front();
@@ -262,39 +333,77 @@ bool admit(eg_server *s, std::unique_lock<std::mutex> &lk)
             break; /* wait for memory to come back */
         }
         if (!g.resident) {
-            eg_game view = g.view();
-            GameLayout L;
+            void *blk = nullptr;
+            const size_t pb = packed_dev_bytes(g.hp);
+            eg_status st = EG_OK;
             lk.unlock();
-            eg_status st = layout_upload(view, s->upload_stream, &L);
+            if (cudaMallocAsync(&blk, pb, s->upload_stream) != cudaSuccess) {
+                cudaGetLastError();
+                st = eg_set_error(EG_ERR_OOM, "device allocation of a game failed");
+            }
+            PackedDev pd;
+            if (st == EG_OK) st = packed_upload(g.hp, blk, s->upload_stream, &pd);
+            if (st == EG_OK && cudaStreamSynchronize(s->upload_stream) != cudaSuccess)
+                st = eg_set_error(EG_ERR_CUDA, "game upload failed");
             lk.lock();
             if (st != EG_OK) {
+                if (blk) cudaFreeAsync(blk, s->upload_stream);
                 s->pending.pop_front();
                 finish_query(s, q, st, clk::now());
                 s->cv_done.notify_all();
                 any = true;
                 continue;
             }
-            g.L = L;
+            g.pd = pd;
             g.resident = true;
             s->uploads++;
-            s->device_bytes += (int64_t)L.bytes;
+            s->device_bytes += (int64_t)pd.bytes;
         }
-        /* one device block per query: credits | thresholds | status | rounds */
+        /* one device block per query: credits | thresholds | MG | rounds | status | scratch */
+        const size_t nu = units.size();
         const size_t fbytes = sizeof(long long) * (size_t)g.n * q.K;
+        const size_t o_thr = (fbytes + 255) & ~(size_t)255;
+        const size_t o_mg = o_thr + (((size_t)q.K * sizeof(int) + 255) & ~(size_t)255);
+        const size_t o_rounds = o_mg + (((size_t)q.K * sizeof(long long) + 255) & ~(size_t)255);
+        const size_t o_status = o_rounds + ((nu * sizeof(long long) + 255) & ~(size_t)255);
+        const size_t o_scr = o_status + ((nu * sizeof(int) + 255) & ~(size_t)255);
+        const size_t total = o_scr + scratch;
         char *blk = nullptr;
-        if (cudaMallocAsync((void **)&blk, query_bytes(g, q.K), s->upload_stream) != cudaSuccess) {
+        if (cudaMallocAsync((void **)&blk, total, s->upload_stream) != cudaSuccess) {
             cudaGetLastError();
             break;
         }
         q.dF = (long long *)blk;
-        q.drounds = (long long *)(blk + fbytes);
-        q.dstatus = (int *)(blk + fbytes + 8);
-        q.dthr = (int *)(blk + fbytes + 16);
-        q.dbytes = query_bytes(g, q.K);
+        q.dthr = (int *)(blk + o_thr);
+        q.dmg = (long long *)(blk + o_mg);
+        q.drounds = (long long *)(blk + o_rounds);
+        q.dstatus = (int *)(blk + o_status);
+        q.dscratch = scratch ? (void *)(blk + o_scr) : nullptr;
+        q.dbytes = total;
+        size_t goff = 0;
+        for (size_t u = 0; u < nu; u++) {
+            UnitDesc &d = units[u];
+            d.E = g.pd.E;
+            d.slice_off = g.pd.slice_off;
+            d.orig = g.pd.orig;
+            d.p = q.dthr;
+            d.mg = q.dmg;
+            d.F = q.dF;
+            d.rounds = q.drounds + u;
+            d.status = q.dstatus + u;
+            if (gneed[u]) {
+                d.gscratch = (char *)q.dscratch + goff;
+                goff += gneed[u];
+            }
+        }
+        q.units.swap(units);
+        q.cost.swap(cost);
+        q.smem = smem;
         cudaMemcpyAsync(q.dthr, q.p.data(), sizeof(int) * (size_t)q.K, cudaMemcpyHostToDevice, s->upload_stream);
+        cudaMemcpyAsync(q.dmg, q.mg.data(), sizeof(long long) * (size_t)q.K, cudaMemcpyHostToDevice, s->upload_stream);
         cudaEventCreateWithFlags(&q.ready, cudaEventDisableTiming);
         cudaEventRecord(q.ready, s->upload_stream);
-        cudaStreamSynchronize(s->upload_stream); /* q.p is host memory that may go away */
+        cudaStreamSynchronize(s->upload_stream); /* q.p / q.mg are host memory that may go away */
         s->device_bytes += (int64_t)q.dbytes;
         g.active++;
         g.last_use = ++s->tick;
@@ -312,48 +421,33 @@ bool admit(eg_server *s, std::unique_lock<std::mutex> &lk)
 bool launch_ready(eg_server *s)
 {
     if (s->ready.empty() || (int)s->inflight.size() >= s->o.streams) return false;
-    std::vector<GameDesc> desc;
-    int kmax = 1, nmax = 32;
-    std::vector<std::pair<long long, int64_t>> order; /* largest game first */
+    std::vector<UnitDesc> all;
+    std::vector<long long> cost;
+    Launch l;
     for (int64_t qid : s->ready) {
         Query &q = *s->queries[qid];
-        ServedGame &g = *s->games[q.game];
-        order.push_back({(long long)g.m * q.K, qid});
+        all.insert(all.end(), q.units.begin(), q.units.end());
+        cost.insert(cost.end(), q.cost.begin(), q.cost.end());
+        l.qids.push_back(qid);
     }
-    std::stable_sort(order.begin(), order.end(), [](auto &a, auto &b) { return a.first > b.first; });
-    Launch l;
-    for (auto &pr : order) {
-        Query &q = *s->queries[pr.second];
-        ServedGame &g = *s->games[q.game];
-        desc.push_back(layout_desc(g.L, q.dthr, q.dF, q.drounds, q.dstatus, q.K, q.d));
-        kmax = std::max(kmax, q.K);
-        nmax = std::max(nmax, g.n);
-        l.qids.push_back(pr.second);
-    }
-    int kp = 1;
-    while (kp < kmax) kp <<= 1;
+    UnitSet S;
+    group_units(all, cost, std::vector<size_t>(all.size(), 0), &S, nullptr);
     l.stream = s->next_stream;
+    l.number = s->micro_batches;
+    l.units = (int)S.units.size();
     s->next_stream = (s->next_stream + 1) % s->o.streams;
     cudaStream_t st = s->streams[l.stream];
     for (int64_t qid : l.qids) cudaStreamWaitEvent(st, s->queries[qid]->ready, 0);
-    cudaError_t e = cudaMallocAsync((void **)&l.ddesc, sizeof(GameDesc) * desc.size(), st);
-    if (e == cudaSuccess) e = cudaMallocAsync((void **)&l.dctrl, sizeof(BatchCtrl), st);
+    cudaError_t e = cudaMallocAsync((void **)&l.dunits, sizeof(UnitDesc) * S.units.size(), st);
+    if (e == cudaSuccess) e = cudaMallocAsync((void **)&l.dctrl, sizeof(UnitCtrl) * kNumVariants, st);
     if (e == cudaSuccess)
-        e = cudaMemcpyAsync(l.ddesc, desc.data(), sizeof(GameDesc) * desc.size(), cudaMemcpyHostToDevice, st);
+        e = cudaMemcpyAsync(l.dunits, S.units.data(), sizeof(UnitDesc) * S.units.size(), cudaMemcpyHostToDevice, st);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&l.ev, cudaEventDisableTiming);
     eg_status ls = EG_OK;
     if (e == cudaSuccess) {
-        BatchParams p;
-        memset(&p, 0, sizeof p);
-        p.games = l.ddesc;
-        p.order = nullptr;
-        p.ctrl = l.dctrl;
-        p.num_games = (int)desc.size();
-        p.words_max = (nmax + 31) / 32;
-        p.max_rounds = s->o.max_rounds;
-        p.timeout_ns = 0;
         int grid = 0;
-        ls = launch_batch(p, kp, s->o.block, s->sms, st, &grid);
+        ls = launch_unit_set(s->launchers[(size_t)l.stream], st, S, l.dunits, l.dctrl, s->o.block, s->sms,
+                             s->o.max_rounds, 0, &grid);
         if (ls == EG_OK) e = cudaEventRecord(l.ev, st);
     }
     if (e != cudaSuccess || ls != EG_OK) {
@@ -368,7 +462,7 @@ bool launch_ready(eg_server *s)
             finish_query(s, q, ls != EG_OK ? ls : EG_ERR_CUDA, now);
         }
         if (l.ev) cudaEventDestroy(l.ev);
-        if (l.ddesc) cudaFreeAsync(l.ddesc, st);
+        if (l.dunits) cudaFreeAsync(l.dunits, st);
         if (l.dctrl) cudaFreeAsync(l.dctrl, st);
         s->ready.clear();
         s->cv_done.notify_all();
@@ -479,6 +573,14 @@ extern "C" eg_status eg_serve_create(const eg_serve_opts *opts, eg_server **out)
     if (s->o.max_rounds == 0) s->o.max_rounds = -1;
     cudaSetDevice(s->o.device);
     cudaDeviceGetAttribute(&s->sms, cudaDevAttrMultiProcessorCount, s->o.device);
+    {
+        eg_status ks = unit_kernel_setup(s->o.device);
+        if (ks != EG_OK) {
+            delete s;
+            return ks;
+        }
+        s->smem_budget = unit_smem_budget(s->o.device);
+    }
     for (int i = 0; i < s->o.streams; i++) {
         cudaStream_t st;
         if (cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) != cudaSuccess) {
@@ -487,8 +589,16 @@ extern "C" eg_status eg_serve_create(const eg_serve_opts *opts, eg_server **out)
             return eg_set_error(EG_ERR_CUDA, "stream creation failed");
         }
         s->streams.push_back(st);
+        s->launchers.emplace_back();
+        if (s->launchers.back().init() != EG_OK) {
+            for (UnitLauncher &L : s->launchers) L.destroy();
+            for (cudaStream_t x : s->streams) cudaStreamDestroy(x);
+            delete s;
+            return eg_set_error(EG_ERR_CUDA, "stream creation failed");
+        }
     }
     if (cudaStreamCreateWithFlags(&s->upload_stream, cudaStreamNonBlocking) != cudaSuccess) {
+        for (UnitLauncher &L : s->launchers) L.destroy();
         for (cudaStream_t x : s->streams) cudaStreamDestroy(x);
         delete s;
         return eg_set_error(EG_ERR_CUDA, "stream creation failed");
@@ -517,6 +627,12 @@ extern "C" eg_status eg_serve_add_game(eg_server *s, const eg_game *game, int64_
         g->has_owner = true;
     }
     g->large = game->num_nodes > kBatchMaxGameNodes;
+    if (!g->large) {
+        /* the packed layout the unit kernel reads (host image, uploaded on admission) */
+        eg_status ps = pack_game(*game, &g->hp);
+        if (ps != EG_OK) return ps;
+        g->fits_smem = (long long)g->hp.rows() * 4 <= (long long)s->smem_budget;
+    }
     std::lock_guard<std::mutex> lk(s->mu);
     g->id = s->next_game++;
     *game_id = g->id;
@@ -533,11 +649,7 @@ extern "C" eg_status eg_serve_remove_game(eg_server *s, int64_t game_id)
     for (auto &kv : s->queries)
         if (kv.second->game == game_id && kv.second->state <= EG_QUERY_RUNNING)
             return eg_set_error(EG_ERR_BUSY, "game %lld still has queries in flight", (long long)game_id);
-    if (it->second->resident) {
-        s->device_bytes -= (int64_t)it->second->L.bytes;
-        layout_free(&it->second->L, s->upload_stream);
-        cudaStreamSynchronize(s->upload_stream);
-    }
+    if (it->second->resident) drop_resident(s, *it->second);
     s->games.erase(it);
     return EG_OK;
 }
@@ -646,6 +758,16 @@ extern "C" eg_status eg_serve_stats_get(eg_server *s, eg_serve_stats *out)
     return EG_OK;
 }
 
+extern "C" eg_status eg_serve_trace(eg_server *s, eg_serve_span *spans, int32_t cap, int32_t *count)
+{
+    if (!s || !count || (cap > 0 && !spans)) return eg_set_error(EG_ERR_INVALID, "NULL argument");
+    std::lock_guard<std::mutex> lk(s->mu);
+    const int32_t n = (int32_t)s->spans.size();
+    for (int32_t i = 0; i < n && i < cap; i++) spans[i] = s->spans[(size_t)i];
+    *count = n;
+    return EG_OK;
+}
+
 extern "C" eg_status eg_serve_destroy(eg_server *s)
 {
     if (!s) return EG_OK;
@@ -659,8 +781,9 @@ extern "C" eg_status eg_serve_destroy(eg_server *s)
     cudaSetDevice(s->o.device);
     for (auto &kv : s->queries) free_query_device(*kv.second, s->upload_stream);
     for (auto &kv : s->games)
-        if (kv.second->resident) layout_free(&kv.second->L, s->upload_stream);
+        if (kv.second->resident && kv.second->pd.block) cudaFreeAsync(kv.second->pd.block, s->upload_stream);
     cudaStreamSynchronize(s->upload_stream);
+    for (UnitLauncher &L : s->launchers) L.destroy();
     for (cudaStream_t st : s->streams) cudaStreamDestroy(st);
     cudaStreamDestroy(s->upload_stream);
     delete s;

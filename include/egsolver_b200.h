@@ -133,7 +133,7 @@ typedef struct eg_opts {
     int32_t dense_depth;         /* chunks in flight per warp in dense rounds: 1 (three
                                     CTAs per SM) or 2 (two CTAs per SM); 0: 2         */
     int32_t dense_sweeps;        /* sweeps of the edge stream per grid barrier in dense
-                                    rounds: 1 or 2; 0: 2                              */
+                                    rounds: 1 to 4; 0: 2                              */
 } eg_opts;
 
 typedef struct eg_stats {
@@ -229,6 +229,25 @@ eg_status eg_dgame_credits_i64(eg_dgame *g, int64_t *credits);
 eg_status eg_dgame_credits_device(eg_dgame *g, void **dev_ptr, int32_t *credit_bits);
 /* Device bytes held by the handle. */
 int64_t eg_dgame_device_bytes(const eg_dgame *g);
+
+/* Autotuner of the AUTO layout (new; the reference picks its kernel from the
+ * command line).  Times capped solves (`rounds` rounds each, from f = 0) of
+ * the resident game, one knob at a time per degree bucket and round kind:
+ * the light/heavy out-degree bound (large_min_deg), the heavy vertices'
+ * task size (task_edges), the thread-per-vertex bucket (small_max_deg), the
+ * sweeps per dense round and the chunks in flight per warp (dense_sweeps,
+ * dense_depth); a value is kept when it lifts edges at least 2% faster.
+ * *tuned receives base with the chosen knobs.  The choice is cached per
+ * game shape (size and out-degree histogram), so a later game of the same
+ * shape takes it without timing.  Every setting gives the same credits. */
+typedef struct eg_tune_report {
+    int32_t candidates;          /* capped solves timed                               */
+    int32_t from_cache;          /* 1: the choice came from the shape cache           */
+    double  default_rate;        /* edge relaxations per ms with base's settings      */
+    double  best_rate;           /* with the chosen settings                          */
+    int32_t reserved[4];
+} eg_tune_report;
+eg_status eg_dgame_tune(eg_dgame *g, const eg_opts *base, int64_t rounds, eg_opts *tuned, eg_tune_report *rep);
 void eg_dgame_free(eg_dgame *g);
 
 /* ------------------------------------------------------------------ */
@@ -251,9 +270,10 @@ eg_status eg_csr2csc_i32(int32_t num_rows, int32_t num_cols, int64_t nnz,
 /* A mean-payoff query "is the mean payoff of v at least p/d?" is the
  * energy game with weights w*d - p (new; the reference solves one energy
  * game per process).  A batch packs many games into one device-resident
- * multi-CSR that their CSC, owners and credits share; one persistent kernel
- * then solves every (game, threshold) pair, one game per CTA with its K
- * thresholds on K lanes, games taken from a device queue largest first. */
+ * layout; one persistent launch then solves every (game, threshold) pair.
+ * The work is cut into units of one game at a group of 1, 2, 4 or 8
+ * thresholds, one CTA per unit with the unit's credits in shared memory,
+ * taken from a device queue heaviest first. */
 #define EG_BATCH_MAX_K 32
 
 typedef struct eg_batch eg_batch;
@@ -267,7 +287,9 @@ typedef struct eg_batch_opts {
     double  timeout_ms;          /* per launch; <= 0: none                          */
     int32_t use_graph;           /* non-zero: the solve's launches are captured in a
                                     CUDA graph on the first solve and replayed      */
-    int32_t reserved[7];
+    int32_t group_max;           /* most thresholds per work unit: 1, 2, 4 or 8
+                                    (0: 8; eg_batch_tune picks one)                 */
+    int32_t reserved[6];
 } eg_batch_opts;
 
 typedef struct eg_batch_stats {
@@ -279,22 +301,27 @@ typedef struct eg_batch_stats {
     int64_t num_top;                 /* (vertex, threshold) pairs at TOP              */
     double  solve_ms;                /* device time of the launch                     */
     int32_t block, grid, games_failed, graph_replayed;
-    int32_t reserved[4];
+    int32_t num_units;               /* work units (game x threshold group)           */
+    int32_t smem_bytes;              /* dynamic shared memory per CTA                 */
+    int32_t reserved[2];
 } eg_batch_stats;
 
-/* Packs and uploads the games (each in eg_game form; all at most 2^19
- * vertices) and builds their CSC on the device. */
+/* Packs the games (each in eg_game form; all at most 2^19 vertices) on the
+ * host cores and uploads them. */
 eg_status eg_batch_create(const eg_game *games, int32_t num_games, const eg_batch_opts *opts, eg_batch **out);
-/* Thresholds p[g*K + k] for every game g and threshold k. */
+/* Thresholds p[g*K + k] for every game g and threshold k; plans the work
+ * units (credit width and threshold groups per game). */
 eg_status eg_batch_set_thresholds(eg_batch *b, const int32_t *p);
 /* Solves every (game, threshold); credits stay on the device. */
 eg_status eg_batch_solve(eg_batch *b, eg_batch_stats *stats);
 /* Credits of one game, threshold-major: credits[k * n_g + v] (TOP = EG_TOP64). */
 eg_status eg_batch_credits(eg_batch *b, int32_t game, int64_t *credits);
-/* Per-game outcome of the last solve: rounds and an eg_status. */
+/* Per-game outcome of the last solve: sweeps (the most of its units) and an
+ * eg_status. */
 eg_status eg_batch_game_result(eg_batch *b, int32_t game, int64_t *rounds, int32_t *status);
-/* Autotuner: times the candidate CTA sizes on the batch's largest games and
- * keeps the fastest for later solves (*block receives it). */
+/* Autotuner: times the candidate CTA sizes and threshold-group sizes on
+ * the whole batch under a sweep cap and keeps the fastest for later solves
+ * (*block receives the CTA size). */
 eg_status eg_batch_tune(eg_batch *b, int32_t *block);
 int64_t eg_batch_device_bytes(const eg_batch *b);
 void eg_batch_free(eg_batch *b);
@@ -365,6 +392,18 @@ eg_status eg_read_game_file(const char *path, const eg_read_opts *ropts, eg_owne
 eg_status eg_read_game_buffer(const char *text, size_t len, const eg_read_opts *ropts, eg_owned_game **out);
 void eg_owned_game_free(eg_owned_game *g);
 
+/* Binary CSR cache (new; the reference re-parses the text every run): the
+ * game as read, with the reader options that shaped it, in one flat file
+ * (64-byte header with a checksum, then row_ptr, succ, weight, ext_id).
+ * eg_read_game_binary rejects a file written with other options (when
+ * ropts != NULL) or whose checksum fails. */
+eg_status eg_write_game_binary(const char *path, const eg_owned_game *g, const eg_read_opts *ropts);
+eg_status eg_read_game_binary(const char *path, const eg_read_opts *ropts, eg_owned_game **out);
+/* eg_read_game_file through a cache: loads cache_path when it is at least as
+ * new as path and matches ropts, else parses path and (re)writes the cache. */
+eg_status eg_read_game_file_cached(const char *path, const eg_read_opts *ropts, const char *cache_path,
+                                   eg_owned_game **out);
+
 /* Streaming form of the same parser: each grammar action calls back, in the
  * order of the reference's parser actions (reference src/the_parser.y:186-301:
  * header, per line node + edges + node_end, footer).  owner is 0 for MAX and
@@ -397,6 +436,22 @@ eg_status eg_read_file_bytes(const char *path, char **buf, size_t *len);
  * Owners are independent fair coins.  Deterministic in `seed`. */
 eg_status eg_generate(int32_t kind, int32_t n, int32_t deg, int32_t wmax, int32_t param,
                       uint64_t seed, eg_owned_game **out);
+
+/* ------------------------------------------------------------------ */
+/* The reference's fixture generators (same text, byte for byte)        */
+/* ------------------------------------------------------------------ */
+
+/* "Clique" game of vertices 0..number-1 (reference script/multi/mkclique.c):
+ * every vertex steps to every other, even ids belong to player 0 (MAX),
+ * odd ids to player 1 (MIN).  *text is malloc'd (eg_free_text). */
+eg_status eg_fixture_clique_text(int32_t number, char **text, size_t *len);
+/* "Ladder" game of 2 * number vertices (reference script/multi/mkladder.c). */
+eg_status eg_fixture_ladder_text(int32_t number, char **text, size_t *len);
+/* `copies` renamed copies of a game given as text, where every vertex of the
+ * first copy also steps to the successors' homologues in every other copy
+ * (reference script/multi/multi.c and the actions of its the_parser.y). */
+eg_status eg_fixture_copies_text(const char *in, size_t in_len, int32_t copies, char **text, size_t *len);
+void eg_free_text(char *text);
 
 #ifdef __cplusplus
 }

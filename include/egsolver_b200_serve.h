@@ -18,13 +18,14 @@ extern "C" {
 
 /* New (the reference is a one-shot command-line program).  A server owns a
  * worker thread that admits queries by free device memory, keeps every
- * admitted game's CSR/CSC resident on the device across its queries, and
+ * admitted game's packed layout resident on the device across its queries, and
  * launches whatever is admitted as one micro-batch while earlier
  * micro-batches still run on other streams, so that their work overlaps on
- * the GPU.  Games of at most 2^19 vertices run in the batched kernel (one
- * CTA per query, K thresholds on K lanes); larger games run one threshold
- * at a time on the persistent grid solver with at most `large_ctas` CTAs,
- * which leaves the remaining SMs to the micro-batches. */
+ * the GPU.  Games of at most 2^19 vertices run in the unit kernel (one CTA
+ * per game x group of thresholds, credits in shared memory); larger games,
+ * and games whose credits miss shared memory while the queue is shallow,
+ * run one threshold at a time on the persistent grid solver with at most
+ * `large_ctas` CTAs, which leaves the remaining SMs to the micro-batches. */
 typedef struct eg_server eg_server;
 
 typedef struct eg_serve_opts {
@@ -48,6 +49,16 @@ typedef struct eg_serve_stats {
     int32_t reserved[6];
 } eg_serve_stats;
 
+/* Device-clock span of one micro-batch (one launch of the unit kernel):
+ * from its first CTA's start to its last CTA's end, in ms since the first
+ * micro-batch's start.  Spans of different micro-batches that intersect
+ * show their work overlapping on the GPU. */
+typedef struct eg_serve_span {
+    int64_t batch;               /* micro-batch number, from 0                */
+    int32_t queries, units;
+    double  begin_ms, end_ms;
+} eg_serve_span;
+
 /* Query states reported by eg_serve_poll. */
 #define EG_QUERY_QUEUED 0
 #define EG_QUERY_RUNNING 1
@@ -69,6 +80,9 @@ eg_status eg_serve_wait(eg_server *s, int64_t query_id, double timeout_ms);
  * query's storage is released afterwards.  *rounds may be NULL. */
 eg_status eg_serve_result(eg_server *s, int64_t query_id, int64_t *credits, int64_t *rounds);
 eg_status eg_serve_stats_get(eg_server *s, eg_serve_stats *stats);
+/* Copies up to cap spans of finished micro-batches; *count receives how
+ * many were recorded. */
+eg_status eg_serve_trace(eg_server *s, eg_serve_span *spans, int32_t cap, int32_t *count);
 /* Stops the worker after the queued queries finished and frees everything. */
 eg_status eg_serve_destroy(eg_server *s);
 

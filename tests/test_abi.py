@@ -131,7 +131,7 @@ def test_bad_options_rejected_before_any_device_work():
     with pytest.raises(eg.EGError):
         eg.solve(g, variant=eg.VARIANT_WARP, lanes_per_vertex=3)
     for bad in (dict(direction=3), dict(direction=-1), dict(dense_permille=1001), dict(sparse_permille=-1),
-                dict(dense_depth=3), dict(dense_depth=-1), dict(dense_sweeps=3), dict(dense_sweeps=-1)):
+                dict(dense_depth=3), dict(dense_depth=-1), dict(dense_sweeps=5), dict(dense_sweeps=-1)):
         with pytest.raises(eg.EGError) as ei:
             eg.solve(g, **bad)
         assert ei.value.name == "EG_ERR_INVALID"

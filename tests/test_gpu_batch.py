@@ -80,6 +80,50 @@ def test_autotuner_then_solve():
         check_batch(b, games, p, 3)
 
 
+def test_unit_variants_match_the_oracle():
+    """Every kind of work unit: 32- and 64-bit credits, 4- and 8-byte slots,
+    groups of 8/4/2/1 thresholds (K = 15 splits into 8 + 4 + 2 + 1), and
+    credits in global scratch for a game too large for shared memory."""
+    rng = np.random.default_rng(21)
+    games = [
+        eg.generate(4, 900, 9, 60, 301, param=2),        # narrow slots, 32-bit credits
+        eg.generate(4, 700, 6, 20000, 302, param=2),     # |w| > 32766 -> 8-byte slots
+        eg.generate(1, 600, 3, 3, 303),                  # tiny weights, big thresholds -> 64-bit credits
+        eg.generate(4, 66000, 3, 5, 304, param=2),       # > 65534 rows -> 8-byte slots, global credits
+    ]
+    d = 3
+    K = 15
+    p = np.zeros((len(games), K), dtype=np.int32)
+    p[0] = rng.integers(-150, 151, K)
+    p[1] = rng.integers(-40000, 40001, K)
+    p[2] = rng.integers(-(1 << 29), 1 << 29, K)         # MG far above 2^30 for positive p
+    p[3] = rng.integers(-12, 13, K)
+    with eg.Batch(games, thresholds=K, scale=d) as b:
+        b.set_thresholds(p)
+        _, st = b.solve()
+        assert st.games_failed == 0
+        assert st.num_units >= 4 * 4
+        for g, game in enumerate(games):
+            got = b.credits(g)
+            for k in range(K):
+                tg = eg.threshold_game(game, int(p[g, k]), d)
+                if game.num_nodes > 10_000:
+                    assert O.count_inconsistent(tg, got[k]) == 0, f"game {g} threshold {k}"
+                else:
+                    want, _ = O.eg_solve(tg, bits=64)
+                    np.testing.assert_array_equal(got[k], want, err_msg=f"game {g} threshold {k}")
+
+
+@pytest.mark.parametrize("group_max", [1, 2, 4, 8])
+def test_group_sizes_give_identical_credits(group_max):
+    games = small_batch(8, seed=31)
+    p = np.random.default_rng(4).integers(-50, 51, size=(len(games), 8)).astype(np.int32)
+    with eg.Batch(games, thresholds=8, scale=2, group_max=group_max) as b:
+        b.set_thresholds(p)
+        b.solve()
+        check_batch(b, games, p, 2)
+
+
 def test_round_cap_marks_games():
     games = [workloads.cfg1()]
     p = np.array([[40]], dtype=np.int32)  # strongly negative weights: long climb to TOP

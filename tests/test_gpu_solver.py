@@ -138,7 +138,8 @@ def test_round_kinds_give_identical_credits(cfg2_2e14, d, bits):
 # or 16-byte edge pairs.
 DENSE_PATHS = [dict(), dict(wide_pairs=True), dict(narrow=True), dict(narrow=True, wide_pairs=True),
                dict(dense_depth=1), dict(dense_depth=1, narrow=True, wide_pairs=True), dict(dense_sweeps=2),
-               dict(dense_sweeps=2, narrow=True, dense_depth=1)]
+               dict(dense_sweeps=2, narrow=True, dense_depth=1), dict(dense_sweeps=3), dict(dense_sweeps=4),
+               dict(dense_sweeps=4, narrow=True, dense_depth=1)]
 
 
 @pytest.mark.parametrize("d", DENSE_PATHS, ids=lambda d: vid(d) or "default")
@@ -363,3 +364,33 @@ def test_ieee1394_model_checking_game(golden_ieee1394):
     game, sol = golden_ieee1394
     f, _ = eg.solve(game, credit_bits=32)
     assert by_ext(game, f) == sol
+
+
+def test_autotuner_keeps_credits_and_caches_by_shape(cfg2_2e14):
+    """Tuned knobs give the oracle's credits; a second game of the same shape
+    takes the cached choice without timing."""
+    game, ref = cfg2_2e14
+    with eg.ResidentGame(game) as r:
+        knobs, rep = r.tune(rounds=120)
+        assert rep["candidates"] >= 5 and not rep["from_cache"]
+        assert rep["best_rate"] >= rep["default_rate"] > 0
+        r.solve(**knobs)
+        np.testing.assert_array_equal(r.credits(64), ref)
+    with eg.ResidentGame(game) as r2:
+        knobs2, rep2 = r2.tune(rounds=120)
+        assert rep2["from_cache"] and knobs2 == knobs
+
+
+def test_autotuner_on_a_game_without_heavy_vertices():
+    """A threshold game of the batched workload (out-degree at most 16, so
+    no heavy tasks; lean kernel and dense rounds) under tuned knobs."""
+    g = workloads.cfg4_games(64)[13]
+    p, d = workloads.cfg4_thresholds(64)
+    tg = eg.threshold_game(g, int(p[13, 0]), d)
+    want, _ = O.eg_solve(tg, bits=64)
+    with eg.ResidentGame(tg) as r:
+        f0, st0 = r.solve()
+        np.testing.assert_array_equal(r.credits(64), want)
+        knobs, rep = r.tune(rounds=200)
+        r.solve(**knobs)
+        np.testing.assert_array_equal(r.credits(64), want)

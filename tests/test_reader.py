@@ -94,3 +94,53 @@ def test_unit_and_random_weight_modes():
     b = eg.read_game_text(text, weight_mode=3, rnd_lo=-4, rnd_hi=4, rnd_seed=9)
     np.testing.assert_array_equal(a.weight, b.weight)
     assert a.weight.min() >= -4 and a.weight.max() <= 4
+
+
+def test_binary_cache_round_trip(tmp_path):
+    """The binary CSR cache gives back the game the text reader gave, and is
+    used (and kept fresh) by the cached reader."""
+    import os
+    import time
+
+    src = tmp_path / "g.txt"
+    src.write_text(eg.copies_text(eg.clique_text(25), 3))
+    want = eg.read_game(str(src))
+    binf = tmp_path / "g.egb"
+    eg.write_game_binary(want, str(binf))
+    got = eg.read_game_binary(str(binf))
+    for a in ("row_ptr", "succ", "weight", "ext_id"):
+        np.testing.assert_array_equal(getattr(got, a), getattr(want, a))
+    assert got.num_nodes0 == want.num_nodes0 and got.max_abs_weight == want.max_abs_weight
+    # options recorded with the file must match when asked for
+    with pytest.raises(eg.EGError):
+        eg.read_game_binary(str(binf), weight_mode=1)
+    # the cached reader writes the cache on first use and reads it afterwards
+    cache = tmp_path / "c.egb"
+    g1 = eg.read_game(str(src), cache=str(cache))
+    assert cache.exists()
+    np.testing.assert_array_equal(g1.succ, want.succ)
+    # a cache that is newer than the text is trusted: prove it by a planted
+    # difference in the text that the cached read does not see
+    src.write_text(eg.clique_text(7))
+    os.utime(cache, (time.time() + 5, time.time() + 5))
+    g2 = eg.read_game(str(src), cache=str(cache))
+    assert g2.num_nodes == want.num_nodes
+    # a newer text replaces the cache
+    os.utime(src, (time.time() + 20, time.time() + 20))
+    g3 = eg.read_game(str(src), cache=str(cache))
+    assert g3.num_nodes == 7
+
+
+def test_binary_file_corruption_is_detected(tmp_path):
+    g = eg.read_game_text(eg.ladder_text(40))
+    p = tmp_path / "x.egb"
+    eg.write_game_binary(g, str(p))
+    raw = bytearray(p.read_bytes())
+    raw[-5] ^= 0x40
+    p.write_bytes(bytes(raw))
+    with pytest.raises(eg.EGError) as ei:
+        eg.read_game_binary(str(p))
+    assert ei.value.name == "EG_ERR_IO"
+    p.write_bytes(bytes(raw[:100]))
+    with pytest.raises(eg.EGError):
+        eg.read_game_binary(str(p))
