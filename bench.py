@@ -58,6 +58,8 @@ ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
 
 METRIC = "EG solve GTEPS (n=2^20, Zipf(2) out-degree, int64 credits)"
+METRICS = {"cfg1": "EG solve GTEPS (n=1000, 4 successors, int64 credits)", "cfg2": METRIC,
+           "cfg3": "EG solve GTEPS (n=2000 clique, int64 credits)"}
 UNIT = "GTEPS"
 
 
@@ -70,14 +72,17 @@ def parse():
     ap.add_argument("--workload", choices=["cfg1", "cfg2", "cfg3", "cfg4", "cfg5"], default="cfg2")
     ap.add_argument("--games", type=int, default=64,
                     help="cfg4: the first G games of the 4096-game stream (same seeds)")
-    ap.add_argument("--plain-sample", type=int, default=24, help="cfg4: (game, threshold) pairs timed on the plain path")
+    ap.add_argument("--plain-sample", type=int, default=0,
+                    help="cfg4: (game, threshold) pairs timed on the plain path (0: all pairs of the batch)")
+    ap.add_argument("--plain-pair-timeout-s", type=float, default=120.0,
+                    help="cfg4: device-side limit of one plain solve (a pair at the limit counts at its limit)")
     ap.add_argument("--batch-timeout-s", type=float, default=120.0,
                     help="cfg4: device-side limit of one batched solve (games still running stop)")
     ap.add_argument("--plain-budget-s", type=float, default=45.0,
                     help="cfg4/cfg5: wall-clock budget of the plain-path measurements")
-    ap.add_argument("--requests", type=int, default=16, help="cfg5: requests per arrival rate (at most)")
-    ap.add_argument("--rates", type=str, default="4,32", help="cfg5: arrival rates (requests/s) swept")
-    ap.add_argument("--n-max", type=int, default=1 << 13, help="cfg5: largest request game")
+    ap.add_argument("--requests", type=int, default=48, help="cfg5: requests per arrival rate (at most)")
+    ap.add_argument("--rates", type=str, default="2,8,32,128,512", help="cfg5: arrival rates (requests/s) swept")
+    ap.add_argument("--n-max", type=int, default=1 << 16, help="cfg5: largest request game")
     ap.add_argument("--n", type=int, default=0, help="override the vertex count (smaller cases)")
     ap.add_argument("--e2e-steps", type=int, default=0, help="e2e steps (default: --steps)")
     ap.add_argument("--cpu-sample-s", type=float, default=10.0)
@@ -312,7 +317,7 @@ def run_reference(args):
     total = sum(times)
     value = edges * args.steps / total / 1e9
     kind = "reference" if use_ref else "port"
-    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+    line = {"impl": "reference", "metric": METRICS[args.workload], "value": value, "unit": UNIT, "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * total / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int32", "data": "synthetic",
             "config": workload_config(args.workload, game, world),
@@ -362,11 +367,11 @@ def progress(msg: str) -> None:
 
 
 def run_batched(args):
-    """cfg4: many uneven games x K=8 mean-payoff thresholds in one persistent
-    launch (CUDA-graph replay, autotuned CTA size) against the plain path that
-    launches the single-game solver once per (game, threshold)."""
-    import torch
-
+    """cfg4: many uneven games x K=8 mean-payoff thresholds in one solve (CUDA
+    graph replay, autotuned units) against the plain path that launches the
+    single-game solver once per (game, threshold), on the same pairs: every
+    pair of the first --games games (--plain-sample 0) or a seeded sample of
+    them.  Each plain solve's credits are compared with the batched ones."""
     import egsolver_b200 as eg
     from egsolver_b200 import workloads
 
@@ -378,7 +383,7 @@ def run_batched(args):
     b = eg.Batch(games, thresholds=K, scale=d, use_graph=True, timeout_ms=1e3 * args.batch_timeout_s)
     b.set_thresholds(p)
     setup_s = time.perf_counter() - t0
-    progress(f"batch of {G} games uploaded in {setup_s:.1f} s")
+    progress(f"batch of {G} games packed and uploaded in {setup_s:.1f} s")
     block = b.tune()
     progress(f"tuned: block {block}")
     for _ in range(args.warmup):
@@ -395,51 +400,63 @@ def run_batched(args):
     ms = sum(times) / len(times)
     done = G - max(s.games_failed for s in stats)  # games solved to the fixed point in every step
     value = done / (ms / 1e3)
-    # parity spot check on the checker: fixed point of a few transformed games
+    batched = {g: b.credits(g) for g in range(G)}
+    status = {g: b.game_result(g)[1] for g in range(G)}
+    last = stats[-1]
+    b.free()
+    # the plain path on the same (game, threshold) pairs: one single-game
+    # solve each, device time; its credits must equal the batched ones
     from oracle import oracle as O
 
     rng = np.random.default_rng(0)
-    for g in rng.choice(G, size=min(8, G), replace=False):
-        if b.game_result(int(g))[1] != 0:
-            continue  # stopped by the time limit: its credits are lower bounds only
-        cr = b.credits(int(g))
-        for k in range(K):
-            tg = eg.threshold_game(games[g], int(p[g, k]), d)
-            if O.count_inconsistent(tg, cr[k]) != 0:
-                raise RuntimeError(f"batched credits of game {g} threshold {k} are not a fixed point")
-    # plain path: one single-game solve per (game, threshold) on a seeded sample
-    pick = rng.choice(G, size=min(args.plain_sample, G), replace=False)
-    plain_ms, plain_pairs = 0.0, 0
+    pairs = [(g, k) for g in range(G) for k in range(K)]
+    if args.plain_sample > 0 and args.plain_sample < len(pairs):
+        pairs = [pairs[i] for i in sorted(rng.choice(len(pairs), size=args.plain_sample, replace=False))]
+    plain_ms, capped, mismatch = 0.0, 0, 0
     t_plain = time.perf_counter()
-    for g in pick:
-        if plain_pairs and time.perf_counter() - t_plain > args.plain_budget_s:
-            break
-        k = int(rng.integers(0, K))
+    for i, (g, k) in enumerate(pairs):
         tg = eg.threshold_game(games[g], int(p[g, k]), d)
         with eg.ResidentGame(tg) as r:
-            status, pst = r.solve(raise_on_error=False, timeout_ms=1e3 * args.batch_timeout_s)
-            if status != 0:
-                progress(f"plain pair: game {g} n={tg.num_nodes} stopped by the time limit")
+            st_, pst = r.solve(raise_on_error=False, timeout_ms=1e3 * args.plain_pair_timeout_s)
+            if st_ != 0:
+                capped += 1  # counted at its time limit: the plain total is a lower bound
+                plain_ms += pst.solve_ms
                 continue
             plain_ms += pst.solve_ms
-            plain_pairs += 1
-            progress(f"plain pair {plain_pairs}: game {g} n={tg.num_nodes} {pst.solve_ms:.1f} ms")
-    plain = plain_pairs / K / (plain_ms / 1e3) if plain_pairs else None
-    last = stats[-1]
-    b.free()
-    line = {"metric": f"batched games/s (cfg4 stream, first {G} of 4096 uneven games x 8 mean-payoff thresholds, "
-                      "one launch)",
+            if status[g] == 0 and not np.array_equal(r.credits(64), batched[g][k]):
+                mismatch += 1
+        if (i + 1) % 32 == 0:
+            progress(f"plain {i + 1}/{len(pairs)} pairs, {plain_ms / 1e3:.1f} s device time so far")
+    plain_wall = time.perf_counter() - t_plain
+    if mismatch:
+        raise RuntimeError(f"{mismatch} plain solves differ from the batched credits")
+    plain = (len(pairs) / K) / (plain_ms / 1e3) if plain_ms > 0 else None
+    # oracle spot check: every threshold of a few small games
+    checked = 0
+    for g in sorted(range(G), key=lambda x: games[x].num_nodes)[:4]:
+        if status[g] != 0:
+            continue
+        for k in range(K):
+            want, _ = O.eg_solve(eg.threshold_game(games[g], int(p[g, k]), d), bits=64)
+            if not np.array_equal(want, batched[g][k]):
+                raise RuntimeError(f"batched credits of game {g} threshold {k} differ from the oracle")
+        checked += 1
+    line = {"metric": f"batched games/s (cfg4 stream, first {G} of 4096 uneven games x {K} mean-payoff thresholds, "
+                      "one solve)",
             "value": value, "unit": "games/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int64",
             "data": "synthetic",
             "games_solved": done, "batch_timeout_s": args.batch_timeout_s,
             "config": {"workload": "batched uneven games", "games": G, "thresholds": K, "d": d,
                        "total_nodes": last.total_nodes, "total_edges": last.total_edges, "block": block,
-                       "graph_replayed": last.graph_replayed, "setup_s": setup_s},
+                       "units": last.num_units, "graph_replayed": last.graph_replayed, "setup_s": setup_s},
             "thresholds_per_s": value * K, "gteps": last.edges / (last.solve_ms * 1e6),
-            "plain": {"games_per_s": plain, "sample_pairs": plain_pairs,
-                      "how": "eg_dgame solve per (game, threshold), device time, seeded sample"},
-            "speedup_vs_plain": value / plain if plain else None, "clocks": clocks,
+            "plain": {"games_per_s": plain, "pairs": len(pairs), "of_pairs": G * K, "device_s": plain_ms / 1e3,
+                      "wall_s": plain_wall, "pairs_at_time_limit": capped,
+                      "pair_time_limit_s": args.plain_pair_timeout_s, "credits_equal_batched": True,
+                      "how": "eg_dgame solve per (game, threshold): transpose, layout and lift per pair, device time"},
+            "speedup_vs_plain": value / plain if plain else None,
+            "oracle_checked_games": checked, "clocks": clocks,
             "solve": {"rounds_max": last.rounds_max, "rounds_sum": last.rounds_sum, "lifts": last.lifts,
                       "edges": last.edges, "num_top": last.num_top, "grid": last.grid}}
     print(json.dumps(line), flush=True)
@@ -447,8 +464,11 @@ def run_batched(args):
 
 def run_served(args):
     """cfg5: Poisson arrivals of mean-payoff threshold queries against the
-    serving loop, rate swept; the plain reference point serves the same
-    arrivals one game at a time (FIFO, service time = measured plain solves)."""
+    serving loop, with the arrival rate swept up to saturation; the plain
+    reference serves the same arrivals one request at a time (FIFO), each
+    request's service time being its measured plain solves (one single-game
+    solve per threshold, device time).  Every served result is compared with
+    the plain credits."""
     import egsolver_b200 as eg
     from egsolver_b200 import workloads
 
@@ -457,20 +477,22 @@ def run_served(args):
     # plain service time of every request: K single-game solves; the stream
     # is cut after the request that exhausts the plain budget, and only the
     # requests measured here are served below
-    plain_service = []
+    plain_service, plain_credits = [], []
     t_plain = time.perf_counter()
     for g, p, d in reqs:
         if plain_service and time.perf_counter() - t_plain > args.plain_budget_s:
             break
-        t = 0.0
-        with eg.ResidentGame(eg.threshold_game(g, int(p[0]), d)) as r:
-            _, st0 = r.solve()
+        t, cr = 0.0, []
         for k in range(len(p)):
-            _, st = eg.solve(eg.threshold_game(g, int(p[k]), d))
-            t += st.solve_ms
+            with eg.ResidentGame(eg.threshold_game(g, int(p[k]), d)) as r:
+                _, st = r.solve()
+                t += st.solve_ms
+                cr.append(r.credits(64))
         plain_service.append(t)
+        plain_credits.append(np.stack(cr))
         progress(f"plain request {len(plain_service)}: n={g.num_nodes} K={len(p)} {t:.1f} ms")
     reqs = reqs[:len(plain_service)]
+    solves = sum(len(p) for _, p, _ in reqs)
     results = []
     for rate in [float(x) for x in args.rates.split(",")]:
         arrivals = np.cumsum(rng.exponential(1.0 / rate, size=len(reqs)))
@@ -485,26 +507,36 @@ def run_served(args):
                 qids.append(srv.submit(gids[i], p, d))
             for q in qids:
                 srv.wait(q, 600_000)
+            for i, q in enumerate(qids):
+                got, _ = srv.result(q)
+                if not np.array_equal(got, plain_credits[i]):
+                    raise RuntimeError(f"served request {i} differs from its plain solves")
             st = srv.stats()
-        progress(f"rate {rate}: p50 {st['latency_p50_ms']:.1f} ms, p99 {st['latency_p99_ms']:.1f} ms")
-        # the same arrivals served one game at a time
+            spans = srv.trace()
+        overlaps = sum(1 for i in range(len(spans)) for j in range(i + 1, len(spans))
+                       if spans[j]["begin_ms"] < spans[i]["end_ms"] and spans[i]["begin_ms"] < spans[j]["end_ms"])
+        progress(f"rate {rate}: {st['solves_per_s']:.1f} solves/s, p50 {st['latency_p50_ms']:.1f} ms, "
+                 f"p99 {st['latency_p99_ms']:.1f} ms, {len(spans)} micro-batches, {overlaps} overlapping pairs")
+        # the same arrivals served one request at a time
         fin, lat = 0.0, []
-        for a, s in zip(arrivals, plain_service):
+        for a, s_ in zip(arrivals, plain_service):
             start = max(a, fin)
-            fin = start + s / 1e3
+            fin = start + s_ / 1e3
             lat.append((fin - a) * 1e3)
-        solves = sum(len(p) for _, p, _ in reqs)
         results.append({"rate": rate, "p50_ms": st["latency_p50_ms"], "p99_ms": st["latency_p99_ms"],
                         "solves_per_s": st["solves_per_s"], "micro_batches": st["micro_batches"],
+                        "overlapping_micro_batch_pairs": overlaps,
                         "plain_p50_ms": float(np.percentile(lat, 50)), "plain_p99_ms": float(np.percentile(lat, 99)),
                         "plain_solves_per_s": solves / fin})
     best = max(results, key=lambda r: r["solves_per_s"])
+    plain_best = solves / (sum(plain_service) / 1e3)  # back-to-back plain solves: its saturated rate
     line = {"metric": "served threshold solves/s with p50/p99 latency (cfg5, Poisson arrivals)",
             "value": best["solves_per_s"], "unit": "solves/s", "n_gpus": 1, "steps": len(results), "warmup": 0,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int64", "data": "synthetic",
             "config": {"workload": "served threshold queries", "requests": len(reqs), "n_max": args.n_max,
-                       "rates": args.rates},
-            "sweep": results}
+                       "rates": args.rates, "thresholds": solves},
+            "plain_saturated_solves_per_s": plain_best, "speedup_vs_plain": best["solves_per_s"] / plain_best,
+            "results_equal_plain": True, "sweep": results}
     print(json.dumps(line), flush=True)
 
 
@@ -538,6 +570,9 @@ def main():
     game = load_workload(args.workload, args.n)
     credit_bits = 64
     cfg = workload_config(args.workload, game, world)
+    if args.variant:
+        cfg["variant"] = {1: "thread per vertex", 2: "warp per vertex (32-lane shuffle reductions)",
+                          3: "CTA per vertex", 4: "one-CTA shared-memory kernel"}[args.variant]
 
     res = eg.ResidentGame(game, device=local)
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.int32, device=f"cuda:{local}")
@@ -677,7 +712,7 @@ def main():
     if rank == 0:
         if capped:
             cfg["profiling_cap_rounds"] = args.max_rounds
-        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        line = {"metric": METRICS[args.workload], "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": dev_ms_max / args.steps, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": f"int{last.credit_bits}", "data": "synthetic",
                 "config": cfg,

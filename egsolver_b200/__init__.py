@@ -312,7 +312,8 @@ class Batch:
     (eg_batch_*).  Threshold p of game g turns every weight w into w*d - p."""
 
     def __init__(self, games: list[Game], thresholds: int, scale: int = 1, block: int = 0, device: int = 0,
-                 max_rounds: int = -1, timeout_ms: float = 0.0, use_graph: bool = False, group_max: int = 0):
+                 max_rounds: int = -1, timeout_ms: float = 0.0, use_graph: bool = False, group_max: int = 0,
+                 tail_rows: int = 0):
         self._h = C.c_void_p()
         self._keep = [g.c_struct() for g in games]
         arr = (_ffi.EgGame * len(games))(*self._keep)
@@ -325,6 +326,7 @@ class Batch:
         o.timeout_ms = timeout_ms
         o.use_graph = 1 if use_graph else 0
         o.group_max = group_max
+        o.tail_rows = tail_rows
         _check(lib().eg_batch_create(arr, len(games), C.byref(o), C.byref(self._h)))
         self.sizes = [g.num_nodes for g in games]
         self.K = thresholds

@@ -126,7 +126,8 @@ class EgBatchOpts(C.Structure):
         ("timeout_ms", C.c_double),
         ("use_graph", C.c_int32),
         ("group_max", C.c_int32),
-        ("reserved", C.c_int32 * 6),
+        ("tail_rows", C.c_int32),
+        ("reserved", C.c_int32 * 5),
     ]
 
 

@@ -34,6 +34,8 @@
  */
 #include "eg_batch.cuh"
 
+#include <cooperative_groups.h>
+
 #include <algorithm>
 #include <atomic>
 #include <cstdio>
@@ -101,6 +103,9 @@ template <> struct Slot<true> {
     }
 };
 
+/* Internal status of a unit handed to the tail (never returned). */
+constexpr int kParked = -1;
+
 struct Shared {
     unsigned raise[3];    /* per-sweep OR of raised thresholds (rotating)     */
     int unit;
@@ -111,10 +116,26 @@ template <int KG> struct Log2 {
     static constexpr int v = KG == 1 ? 0 : KG == 2 ? 1 : KG == 4 ? 2 : 3;
 };
 
+/* Where a unit's credits live: all rows in shared memory, or (HYB, a
+ * hybrid unit) rows below S there and the rest in the unit's global
+ * scratch, which only the owning CTA touches. */
+template <int KG, typename CT, bool HYB>
+struct Cred {
+    CT *Fs;
+    CT *Fg;
+    int S;
+    __device__ __forceinline__ CT *at(int row) const
+    {
+        if (!HYB || row < S) return Fs + ((long long)row << Log2<KG>::v);
+        return Fg + ((long long)(row - S) << Log2<KG>::v);
+    }
+};
+
 /* min (player 0) or max (player 1, MAXV) over the W columns of a slice of
  * credit - w * d, for the KG thresholds at once; lane's first slot at i0. */
-template <int KG, typename CT, bool WIDE, bool MAXV, int UNR>
-__device__ __forceinline__ void column_walk(const void *E, int i0, int W, const CT *F, CT d, CT (&acc)[KG])
+template <int KG, typename CT, bool WIDE, bool MAXV, int UNR, bool HYB>
+__device__ __forceinline__ void column_walk(const void *E, int i0, int W, const Cred<KG, CT, HYB> &F, CT d,
+                                            CT (&acc)[KG])
 {
     using S = Slot<WIDE>;
     using ST = typename S::T;
@@ -134,7 +155,7 @@ __device__ __forceinline__ void column_walk(const void *E, int i0, int W, const 
             if (c + x < W) {
                 int sc;
                 S::dec(q[x], sc, wt[x]);
-                fr[x] = *(const R *)(F + ((long long)sc << LK));
+                fr[x] = *(const R *)F.at(sc);
             }
         }
 #pragma unroll
@@ -152,11 +173,12 @@ __device__ __forceinline__ void column_walk(const void *E, int i0, int W, const 
 }
 
 /* Solves one unit (KG thresholds, credit type CT, slot width WIDE, credits
- * in shared memory or, with GF, in the unit's global scratch). */
+ * in shared memory or, with GF (a hybrid unit, KG = 1), rows from u.srows on
+ * in the unit's global scratch). */
 template <int KG, typename CT, bool WIDE, bool GF>
-__device__ __forceinline__ void run_unit(const UnitDesc &u, unsigned char *smem, Shared &sh, const UnitParams &P,
-                                      unsigned long long t0, unsigned long long &lifts, unsigned long long &edges,
-                                      unsigned long long &ntop)
+__device__ __forceinline__ void run_unit(const UnitDesc &u, int uglobal, unsigned char *smem, Shared &sh,
+                                         const UnitParams &P, unsigned long long t0, unsigned long long &lifts,
+                                         unsigned long long &edges, unsigned long long &ntop)
 {
     using R = Row<KG, CT>;
     constexpr CT TOPI = Lim<CT>::top, LOWI = Lim<CT>::low;
@@ -165,12 +187,15 @@ __device__ __forceinline__ void run_unit(const UnitDesc &u, unsigned char *smem,
     constexpr int UNR = (KG * (int)sizeof(CT) <= 4) ? 8 : (KG * (int)sizeof(CT) <= 8) ? 4
                         : (KG * (int)sizeof(CT) <= 16) ? 2 : 1;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nwarps = blockDim.x >> 5;
-    CT *F = GF ? (CT *)u.gscratch : (CT *)smem;
+    Cred<KG, CT, GF> F;
+    F.Fs = (CT *)smem;
+    F.Fg = (CT *)u.gscratch;
+    F.S = GF ? u.srows : 0;
     const int ns = u.ns, s0 = u.s0, npad = 32 * ns;
     const int rows = npad + 2;
     for (int i = tid; i < rows * KG; i += blockDim.x) {
         const int r = i >> LK;
-        F[i] = r < npad ? (CT)0 : (r == npad ? TOPI : LOWI);
+        F.at(r)[i & (KG - 1)] = r < npad ? (CT)0 : (r == npad ? TOPI : LOWI);
     }
     if (tid < KG) {
         sh.p[tid] = u.p[u.k0 + tid];
@@ -190,12 +215,13 @@ __device__ __forceinline__ void run_unit(const UnitDesc &u, unsigned char *smem,
             const int W = (__ldg(u.slice_off + s + 1) - b) >> 5;
             const bool own1 = s >= s0;
             CT acc[KG];
-            if (own1) column_walk<KG, CT, WIDE, true, UNR>(u.E, b + lane, W, F, d, acc);
-            else column_walk<KG, CT, WIDE, false, UNR>(u.E, b + lane, W, F, d, acc);
+            if (own1) column_walk<KG, CT, WIDE, true, UNR, GF>(u.E, b + lane, W, F, d, acc);
+            else column_walk<KG, CT, WIDE, false, UNR, GF>(u.E, b + lane, W, F, d, acc);
             const int v = 32 * s + lane;
             const bool real = own1 ? (v - 32 * s0 < u.n1) : (v < u.n0);
             if (real) {
-                R old = *(const R *)(F + ((long long)v << LK));
+                CT *mine = F.at(v);
+                R old = *(const R *)mine;
 #pragma unroll
                 for (int k = 0; k < KG; k++) {
                     if (amask >> k & 1u) {
@@ -203,7 +229,7 @@ __device__ __forceinline__ void run_unit(const UnitDesc &u, unsigned char *smem,
                         const CT val = acc[k] + (CT)sh.p[k];
                         const CT nv = val > (CT)sh.mg[k] ? TOPI : (val > 0 ? val : (CT)0);
                         if (nv > old.v[k]) {
-                            F[((long long)v << LK) + k] = nv;
+                            mine[k] = nv;
                             raised |= 1u << k;
                         }
                     }
@@ -213,7 +239,15 @@ __device__ __forceinline__ void run_unit(const UnitDesc &u, unsigned char *smem,
         raised = __reduce_or_sync(0xffffffffu, raised);
         const int slot = (int)(r % 3);
         if (lane == 0 && raised) atomicOr(&sh.raise[slot], raised);
-        if (tid == 0 && P.timeout_ns && globaltimer_ns() - t0 > P.timeout_ns) atomicOr(&sh.raise[slot], 1u << 16);
+        if (tid == 0) {
+            if (P.timeout_ns && globaltimer_ns() - t0 > P.timeout_ns) atomicOr(&sh.raise[slot], 1u << 16);
+            /* park: this variant's queue is empty and half of all phase-1
+             * CTAs have nothing left, so the GPU is running the tail; the
+             * unit's open thresholds continue on clusters */
+            if (P.tails && (r & 15) == 15 && ld_volatile(&P.ctrl->next) >= P.num_units &&
+                2 * ld_volatile(P.idle) >= P.park_total)
+                atomicOr(&sh.raise[slot], 1u << 17);
+        }
         __syncthreads();
         const unsigned word = sh.raise[slot];
         if (tid == 0) {
@@ -224,8 +258,12 @@ __device__ __forceinline__ void run_unit(const UnitDesc &u, unsigned char *smem,
         r++;
         amask &= word & full;
         if (amask == 0) break;
-        if (word >> 16) {
+        if (word & (1u << 16)) {
             st = EG_ERR_TIMEOUT;
+            break;
+        }
+        if (word & (1u << 17)) {
+            st = kParked;
             break;
         }
         if (P.max_rounds >= 0 && r >= P.max_rounds) {
@@ -240,15 +278,34 @@ __device__ __forceinline__ void run_unit(const UnitDesc &u, unsigned char *smem,
         const int k = i / npad, v = i - k * npad;
         const int o = __ldg(u.orig + v);
         if (o >= 0) {
-            const CT c = F[((long long)v << LK) + k];
+            const CT c = F.at(v)[k];
             u.F[(long long)(u.k0 + k) * u.n + o] = c >= TOPI ? (long long)INT64_MAX : (long long)c;
-            top += c >= TOPI;
+            /* the TOPs of a parked unit's open thresholds are counted by the tail */
+            top += c >= TOPI && !(st == kParked && (amask >> k & 1u));
         }
     }
     ntop += top;
+    if (tid == 0) sh.unit = 0; /* reused below as the overflow flag */
+    __syncthreads();
+    if (st == kParked && tid < KG && (amask >> tid & 1u)) {
+        TailList *tl = P.tails + tail_class(u.variant);
+        const int at = atomicAdd(&tl->count, 1);
+        if (at < tl->cap) {
+            TailEntry e;
+            e.unit = uglobal;
+            e.k = u.k0 + tid;
+            e.sweeps = r;
+            e.resume = 1;
+            e.pad = 0;
+            tl->e[at] = e;
+        } else {
+            atomicExch(&sh.unit, 1); /* cannot happen: lists hold every threshold */
+        }
+    }
+    __syncthreads();
     if (tid == 0) {
         *u.rounds = r;
-        *u.status = st;
+        *u.status = sh.unit ? EG_ERR_OOM : (st == kParked ? EG_OK : st);
     }
     __syncthreads();
 }
@@ -260,8 +317,14 @@ __global__ void __launch_bounds__(1024, 1) k_units(const __grid_constant__ UnitP
 {
     extern __shared__ __align__(16) unsigned char smem[];
     __shared__ Shared sh;
-    const unsigned long long t0 = globaltimer_ns(); /* this CTA's start */
-    if (threadIdx.x == 0) atomicCAS(&P.ctrl->t_begin, 0ull, t0);
+    if (threadIdx.x == 0) {
+        const unsigned long long now = globaltimer_ns();
+        atomicCAS(&P.ctrl->t_begin, 0ull, now);
+        atomicCAS(P.t_start, 0ull, now);
+    }
+    __syncthreads();
+    /* timeouts count from the launch's first CTA (phase 1 or tail) */
+    const unsigned long long t0 = ld_volatile_u64(P.t_start);
     unsigned long long lifts = 0, edges = 0, ntop = 0;
     for (;;) {
         if (threadIdx.x == 0) sh.unit = atomicAdd(&P.ctrl->next, 1);
@@ -270,8 +333,9 @@ __global__ void __launch_bounds__(1024, 1) k_units(const __grid_constant__ UnitP
         __syncthreads();
         if (ui >= P.num_units) break;
         const UnitDesc u = P.units[ui];
-        run_unit<KG, CT, WIDE, GF>(u, smem, sh, P, t0, lifts, edges, ntop);
+        run_unit<KG, CT, WIDE, GF>(u, P.unit_base + ui, smem, sh, P, t0, lifts, edges, ntop);
     }
+    if (threadIdx.x == 0 && P.idle) atomicAdd(P.idle, 1);
     const int lane = threadIdx.x & 31;
 #pragma unroll
     for (int off = 16; off > 0; off >>= 1) ntop += __shfl_xor_sync(0xffffffffu, ntop, off);
@@ -313,6 +377,241 @@ unit_kernel_t kernel_of(int v)
     default: return nullptr;
     }
 #undef EG_K
+}
+
+
+/* ------------------------------------------------------------------ */
+/* The tail: one (unit, threshold) per thread-block cluster             */
+/* ------------------------------------------------------------------ */
+
+namespace cg = cooperative_groups;
+
+/* Every CTA of the cluster holds a full replica of the unit's credits in
+ * its shared memory and lifts the slices of its own row range [rank * R,
+ * (rank + 1) * R) (R = ceil(rows / cluster size) rounded up to 32, so a
+ * slice never straddles two ranges), gathering successor credits from its
+ * local replica.  At the end of a sweep a CTA that raised a credit pushes
+ * its own range into every peer's replica (16-byte stores through the
+ * cluster's distributed shared memory), and a cluster barrier makes those
+ * writes visible before the next sweep.  A CTA thus reads its peers'
+ * credits as of the previous sweep's end: values below the least fixed
+ * point, so the iteration stays a fair chaotic one; a sweep in which no CTA
+ * raised anything leaves all replicas equal and every vertex lifted against
+ * them, i.e. the least fixed point.  The OR of the CTAs' raise flags is
+ * gathered in rank 0's shared memory (three rotating words, as in phase 1).
+ * Random 4-byte gathers through distributed shared memory are about ten
+ * times slower than local ones, hence the replicas. */
+template <typename CT, bool WIDE, bool HYB>
+__global__ void __launch_bounds__(1024, 1) k_tail(const __grid_constant__ TailParams T)
+{
+    using S = Slot<WIDE>;
+    using ST = typename S::T;
+    constexpr CT TOPI = Lim<CT>::top, LOWI = Lim<CT>::low;
+    constexpr int UNR = sizeof(CT) == 4 ? 8 : 4;
+    constexpr int VEC = 16 / (int)sizeof(CT); /* credits per 16-byte store */
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    CT *F = (CT *)smem_raw;
+    __shared__ int s_entry;
+    __shared__ unsigned s_word[3];
+    cg::cluster_group cl = cg::this_cluster();
+    const int rank = (int)cl.block_rank();
+    const int C = (int)cl.num_blocks();
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nwarps = blockDim.x >> 5;
+    /* hybrid: rows >= srows of this CTA's replica live in its own global
+     * region, which its peers write at sweep ends (read through L2) */
+    CT *G = HYB ? (CT *)(T.gscratch + (long long)blockIdx.x * T.gstride) : nullptr;
+    if (tid == 0) {
+        const unsigned long long now = globaltimer_ns();
+        atomicCAS(&T.ctrl->t_begin, 0ull, now);
+        atomicCAS(T.t_start, 0ull, now);
+    }
+    __syncthreads();
+    const unsigned long long t0 = ld_volatile_u64(T.t_start);
+    unsigned long long lifts = 0, edges = 0, ntop = 0;
+    for (;;) {
+        if (rank == 0 && tid == 0) s_entry = atomicAdd(&T.list->next, 1);
+        cl.sync();
+        const int ei = *cl.map_shared_rank(&s_entry, 0);
+        cl.sync();
+        if (ei >= T.list->count || ei >= T.list->cap) break;
+        const TailEntry en = T.list->e[ei];
+        const UnitDesc u = T.units[en.unit];
+        const int k = en.k;
+        const int npad = 32 * u.ns, rows = npad + 2;
+        const int SR = HYB ? u.srows : rows; /* rows in shared memory */
+        const int R = (((rows + C - 1) / C) + 31) & ~31;
+        const int lo = min(rows, rank * R);
+        const int hi = min(npad, lo + R); /* own rows */
+        auto ld = [&](int row) -> CT { return (!HYB || row < SR) ? F[row] : (CT)__ldcg(G + (row - SR)); };
+        auto stv = [&](int row, CT x) {
+            if (!HYB || row < SR) F[row] = x;
+            else __stcg(G + (row - SR), x);
+        };
+        /* the full replica */
+        for (int v = tid; v < rows; v += blockDim.x) {
+            CT x;
+            if (v == npad) x = TOPI;
+            else if (v == npad + 1) x = LOWI;
+            else {
+                x = 0;
+                const int o = __ldg(u.orig + v);
+                if (en.resume && o >= 0) {
+                    const long long c = u.F[(long long)k * u.n + o];
+                    x = c == (long long)INT64_MAX ? TOPI : (CT)c;
+                }
+            }
+            stv(v, x);
+        }
+        const CT pk = (CT)u.p[k], mgk = (CT)u.mg[k], d = (CT)u.d;
+        if (tid == 0) s_word[0] = s_word[1] = s_word[2] = 0u;
+        cl.sync();
+        long long r = 0;
+        int st = EG_OK;
+        const int s_lo = lo >> 5, s_hi = hi >> 5;
+        for (;;) {
+            unsigned raised = 0;
+            for (int s = s_lo + warp; s < s_hi; s += nwarps) {
+                const int b = __ldg(u.slice_off + s);
+                const int W = (__ldg(u.slice_off + s + 1) - b) >> 5;
+                const bool own1 = s >= u.s0;
+                CT acc = own1 ? Lim<CT>::lo_acc : Lim<CT>::hi_acc;
+                for (int c = 0; c < W; c += UNR) {
+                    ST q[UNR];
+#pragma unroll
+                    for (int x = 0; x < UNR; x++)
+                        if (c + x < W) q[x] = S::load(u.E, b + lane + 32 * (c + x));
+                    CT f[UNR];
+                    int wt[UNR];
+#pragma unroll
+                    for (int x = 0; x < UNR; x++) {
+                        if (c + x < W) {
+                            int sc;
+                            S::dec(q[x], sc, wt[x]);
+                            f[x] = ld(sc);
+                        }
+                    }
+#pragma unroll
+                    for (int x = 0; x < UNR; x++) {
+                        if (c + x < W) {
+                            const CT y = f[x] - (CT)wt[x] * d;
+                            acc = own1 ? (y > acc ? y : acc) : (y < acc ? y : acc);
+                        }
+                    }
+                }
+                const int v = 32 * s + lane;
+                const bool real = own1 ? (v - 32 * u.s0 < u.n1) : (v < u.n0);
+                if (real) {
+                    const CT val = acc + pk;
+                    const CT nv = val > mgk ? TOPI : (val > 0 ? val : (CT)0);
+                    if (nv > ld(v)) {
+                        stv(v, nv);
+                        raised = 1u;
+                    }
+                }
+            }
+            const int slot = (int)(r % 3);
+            const int any = __syncthreads_or((int)raised);
+            if (any) {
+                /* push the own range into every peer's replica: the part in
+                 * shared memory through distributed shared memory, the part
+                 * in global memory into the peer's region */
+                const int mid = max(lo, min(hi, SR));
+                const int nsv = (mid - lo) / VEC, ngv = (hi - mid) / VEC;
+                const int4 *ssrc = (const int4 *)(F + lo);
+                const int4 *gsrc = HYB ? (const int4 *)(G + (mid - SR)) : nullptr;
+                for (int q = 1; q < C; q++) {
+                    const int peer = (rank + q) % C;
+                    int4 *sdst = (int4 *)cl.map_shared_rank(F + lo, peer);
+                    for (int i = tid; i < nsv; i += blockDim.x) sdst[i] = ssrc[i];
+                    if (HYB && ngv > 0) {
+                        int4 *gdst = (int4 *)(T.gscratch + (long long)(blockIdx.x - rank + peer) * T.gstride) +
+                                     (mid - SR) / VEC;
+                        for (int i = tid; i < ngv; i += blockDim.x) __stcg(gdst + i, __ldcg(gsrc + i));
+                    }
+                }
+                if (tid == 0) atomicOr(cl.map_shared_rank(&s_word[slot], 0), 1u);
+            }
+            if (rank == 0 && tid == 0 && T.timeout_ns && globaltimer_ns() - t0 > T.timeout_ns)
+                atomicOr(&s_word[slot], 1u << 16);
+            cl.sync();
+            const unsigned word = *cl.map_shared_rank(&s_word[slot], 0);
+            if (rank == 0 && tid == 0) {
+                s_word[(r + 2) % 3] = 0u;
+                lifts += (unsigned long long)(u.n0 + u.n1);
+                edges += (unsigned long long)u.m;
+            }
+            r++;
+            if (!(word & 1u)) break;
+            if (word & (1u << 16)) {
+                st = EG_ERR_TIMEOUT;
+                break;
+            }
+            if (T.max_rounds >= 0 && en.sweeps + r >= T.max_rounds) {
+                st = EG_ERR_LOOPCAP;
+                break;
+            }
+        }
+        /* credits out (own rows), TOP count, the unit's sweeps and status */
+        unsigned long long top = 0;
+        for (int v = lo + tid; v < hi; v += blockDim.x) {
+            const int o = __ldg(u.orig + v);
+            if (o >= 0) {
+                const CT c = ld(v);
+                u.F[(long long)k * u.n + o] = c >= TOPI ? (long long)INT64_MAX : (long long)c;
+                top += c >= TOPI;
+            }
+        }
+        ntop += top;
+        if (rank == 0 && tid == 0) {
+            atomicMax((unsigned long long *)u.rounds, (unsigned long long)(en.sweeps + r));
+            if (st != EG_OK) atomicExch(u.status, st);
+        }
+        cl.sync(); /* no CTA writes into another's replica of this entry any more */
+    }
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) ntop += __shfl_xor_sync(0xffffffffu, ntop, off);
+    if (lane == 0 && ntop) atomicAdd(&T.ctrl->num_top, ntop);
+    if (tid == 0) {
+        atomicAdd(&T.ctrl->lifts, lifts);
+        atomicAdd(&T.ctrl->edges, edges);
+        atomicMax(&T.ctrl->t_end, globaltimer_ns());
+    }
+}
+
+typedef void (*tail_kernel_t)(TailParams);
+
+tail_kernel_t tail_kernel_of(int cls)
+{
+    switch (cls) {
+    case 0: return (tail_kernel_t)k_tail<int, false, false>;
+    case 1: return (tail_kernel_t)k_tail<long long, false, false>;
+    case 2: return (tail_kernel_t)k_tail<int, true, false>;
+    case 3: return (tail_kernel_t)k_tail<long long, true, false>;
+    case 4: return (tail_kernel_t)k_tail<int, false, true>;
+    case 5: return (tail_kernel_t)k_tail<long long, false, true>;
+    case 6: return (tail_kernel_t)k_tail<int, true, true>;
+    default: return (tail_kernel_t)k_tail<long long, true, true>;
+    }
+}
+
+/* Before a solve: rewinds the tail lists to their host-listed entries and
+ * clears the sweeps and status of the units those entries belong to (no
+ * phase-1 kernel writes them). */
+__global__ void k_tail_rewind(TailList *lists, const UnitDesc *units)
+{
+    for (int c = 0; c < kTailClasses; c++) {
+        const TailList &l = lists[c];
+        for (int i = threadIdx.x; i < l.init; i += blockDim.x) {
+            const UnitDesc &u = units[l.e[i].unit];
+            *u.rounds = 0;
+            *u.status = EG_OK;
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x < kTailClasses) {
+        lists[threadIdx.x].count = lists[threadIdx.x].init;
+        lists[threadIdx.x].next = 0;
+    }
 }
 
 int align32i(int x) { return (x + 31) & ~31; }
@@ -462,19 +761,25 @@ bool credits32_ok(const HostPacked &h, const int *p, int K, int d, const long lo
     return true;
 }
 
-UnitPlan plan_game(const HostPacked &h, bool credit64, int smem_budget, int kg_cap)
+int tail_rows_per_cta(int rows) { return (rows + 31) & ~31; }
+
+UnitPlan plan_game(const HostPacked &h, bool credit64, int smem_budget, int kg_cap, int tail_rows)
 {
     UnitPlan pl;
     pl.credit64 = credit64 ? 1 : 0;
     pl.kg_max = 0;
+    pl.tail = 0;
     const long long cb = credit64 ? 8 : 4;
     for (int kg = 8; kg >= 1; kg >>= 1) {
+        if (tail_rows > 0 && h.n >= tail_rows) break;
         if (kg > kg_cap) continue;
         if ((long long)h.rows() * kg * cb <= smem_budget) {
             pl.kg_max = kg;
-            break;
+            return pl;
         }
     }
+    /* too large for one CTA: a cluster holds it, else global scratch */
+    pl.tail = (long long)tail_rows_per_cta(h.rows()) * cb <= smem_budget ? 1 : 0;
     return pl;
 }
 
@@ -493,16 +798,41 @@ void split_thresholds(int K, int kg_max, std::vector<std::pair<int, int>> *group
 eg_status make_units(const HostPacked &h, const PackedDev &pd, int K, int d, const int *p, const long long *mg,
                      const int *p_dev, const long long *mg_dev, long long *F_dev, int smem_budget, int kg_cap,
                      std::vector<UnitDesc> *units, std::vector<size_t> *gneed, std::vector<long long> *cost,
-                     int *smem)
+                     int *smem, int tail_rows)
 {
     if ((long long)h.wpad * d >= (1LL << 31))
         return eg_set_error(EG_ERR_OVERFLOW, "weight * scale does not fit 32 bits");
     for (int k = 0; k < K; k++)
         if (mg[k] >= (1LL << 61)) return eg_set_error(EG_ERR_OVERFLOW, "threshold %d: MG %lld too large", k, mg[k]);
     const bool c64 = !credits32_ok(h, p, K, d, mg);
-    const UnitPlan pl = plan_game(h, c64, smem_budget, kg_cap);
+    const UnitPlan pl = plan_game(h, c64, smem_budget, kg_cap, tail_rows);
     std::vector<std::pair<int, int>> groups;
     split_thresholds(K, pl.kg_max, &groups);
+    if (pl.tail) {
+        /* one unit for all thresholds: the host lists (unit, k) for every k */
+        UnitDesc u;
+        memset(&u, 0, sizeof u);
+        u.E = pd.E;
+        u.slice_off = pd.slice_off;
+        u.orig = pd.orig;
+        u.p = p_dev;
+        u.mg = mg_dev;
+        u.F = F_dev;
+        u.m = h.m;
+        u.n = h.n;
+        u.n0 = h.n0;
+        u.n1 = h.n1;
+        u.ns = h.ns;
+        u.s0 = h.s0;
+        u.d = d;
+        u.k0 = 0;
+        u.pad = K; /* thresholds to list */
+        u.variant = kUnitTail | (c64 ? kUnitCredit64 : 0) | (h.wide ? kUnitWide : 0);
+        units->push_back(u);
+        gneed->push_back(0);
+        cost->push_back(h.m * (long long)h.n * K);
+        return EG_OK;
+    }
     for (auto &gr : groups) {
         UnitDesc u;
         memset(&u, 0, sizeof u);
@@ -523,8 +853,13 @@ eg_status make_units(const HostPacked &h, const PackedDev &pd, int K, int d, con
         const int kg = 1 << gr.second;
         const size_t need = (size_t)h.rows() * kg * (c64 ? 8 : 4);
         if (pl.kg_max == 0) {
+            /* hybrid: as many rows as fit in shared memory, the rest in the
+             * unit's global scratch */
+            const int cb = c64 ? 8 : 4;
             u.variant = (c64 ? kUnitCredit64 : 0) | (h.wide ? kUnitWide : 0) | kUnitGlobal;
-            gneed->push_back((need + 255) & ~(size_t)255);
+            u.srows = std::max(32, (smem_budget / cb) & ~31);
+            gneed->push_back(((size_t)(h.rows() - u.srows) * cb + 255) & ~(size_t)255);
+            *smem = std::max(*smem, u.srows * cb);
         } else {
             u.variant = gr.second | (c64 ? kUnitCredit64 : 0) | (h.wide ? kUnitWide : 0);
             gneed->push_back(0);
@@ -552,6 +887,12 @@ int unit_smem_budget(int device)
         if (cudaFuncGetAttributes(&fa, (const void *)k) != cudaSuccess) cudaGetLastError();
         stat = std::max(stat, (int)fa.sharedSizeBytes);
     }
+    for (int c = 0; c < kTailClasses; c++) {
+        cudaFuncAttributes fa;
+        memset(&fa, 0, sizeof fa);
+        if (cudaFuncGetAttributes(&fa, (const void *)tail_kernel_of(c)) != cudaSuccess) cudaGetLastError();
+        stat = std::max(stat, (int)fa.sharedSizeBytes);
+    }
     return optin - stat - 64;
 }
 
@@ -564,6 +905,11 @@ eg_status unit_kernel_setup(int device)
         cudaError_t e = cudaFuncSetAttribute((const void *)k, cudaFuncAttributeMaxDynamicSharedMemorySize, budget);
         if (e != cudaSuccess) return eg_set_error(EG_ERR_CUDA, "cudaFuncSetAttribute failed: %s", cudaGetErrorString(e));
     }
+    for (int c = 0; c < kTailClasses; c++) {
+        cudaError_t e = cudaFuncSetAttribute((const void *)tail_kernel_of(c), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             budget);
+        if (e != cudaSuccess) return eg_set_error(EG_ERR_CUDA, "cudaFuncSetAttribute failed: %s", cudaGetErrorString(e));
+    }
     return EG_OK;
 }
 
@@ -573,6 +919,7 @@ void group_units(const std::vector<UnitDesc> &units, const std::vector<long long
     const int nu = (int)units.size();
     std::vector<int> order((size_t)nu);
     std::iota(order.begin(), order.end(), 0);
+    /* phase-1 units by variant, heaviest first; tail units last */
     std::stable_sort(order.begin(), order.end(), [&](int a, int c) {
         if (units[(size_t)a].variant != units[(size_t)c].variant)
             return units[(size_t)a].variant < units[(size_t)c].variant;
@@ -584,17 +931,45 @@ void group_units(const std::vector<UnitDesc> &units, const std::vector<long long
         S.smem[v] = 16;
         S.top_cost[v] = -1;
     }
+    for (int c = 0; c < kTailClasses; c++) {
+        S.tail_cap[c] = 0;
+        S.tail_smem[c] = 16;
+        S.tail_gbytes[c] = 0;
+    }
     for (int i : order) {
         const UnitDesc &u = units[(size_t)i];
         const int v = u.variant;
+        const int j = (int)S.units.size();
         S.units.push_back(u);
         S.gneed.push_back(gneed[(size_t)i]);
+        const int cls = tail_class(v);
+        const int rows = 32 * u.ns + 2;
+        const int cb = (v & kUnitCredit64) ? 8 : 4;
+        if (v & kUnitTail) {
+            for (int k = 0; k < u.pad; k++) {
+                TailEntry e;
+                memset(&e, 0, sizeof e);
+                e.unit = j;
+                e.k = k;
+                S.tail_init[cls].push_back(e);
+            }
+            S.tail_cap[cls] += u.pad;
+            S.tail_smem[cls] = std::max(S.tail_smem[cls], tail_rows_per_cta(rows) * cb);
+            continue;
+        }
         S.off[v + 1]++;
         S.top_cost[v] = std::max(S.top_cost[v], cost[(size_t)i]);
+        /* a parked unit lists its open thresholds for the tail */
         if (!(v & kUnitGlobal)) {
             const int kg = 1 << (v & kUnitKgMask);
-            const int need = (32 * u.ns + 2) * kg * ((v & kUnitCredit64) ? 8 : 4);
-            S.smem[v] = std::max(S.smem[v], need);
+            S.smem[v] = std::max(S.smem[v], rows * kg * cb);
+            S.tail_cap[cls] += kg;
+            S.tail_smem[cls] = std::max(S.tail_smem[cls], tail_rows_per_cta(rows) * cb);
+        } else {
+            S.smem[v] = std::max(S.smem[v], u.srows * cb);
+            S.tail_cap[cls] += 1;
+            S.tail_smem[cls] = std::max(S.tail_smem[cls], u.srows * cb);
+            S.tail_gbytes[cls] = std::max(S.tail_gbytes[cls], ((long long)(rows - u.srows) * cb + 255) & ~255LL);
         }
     }
     for (int v = 0; v < kNumVariants; v++) S.off[v + 1] += S.off[v];
@@ -602,12 +977,56 @@ void group_units(const std::vector<UnitDesc> &units, const std::vector<long long
     *out = std::move(S);
 }
 
+static size_t al16(size_t x) { return (x + 15) & ~(size_t)15; }
+
+/* Clusters a hybrid tail class launches (its scratch holds that many). */
+static int tail_hyb_clusters(int num_sms) { return num_sms / kTailCluster + 1; }
+
+size_t tail_scratch_bytes(const UnitSet &S, int num_sms)
+{
+    size_t b = 0;
+    for (int c = 0; c < kTailClasses; c++)
+        if (S.tail_cap[c] > 0 && S.tail_gbytes[c] > 0)
+            b += (size_t)tail_hyb_clusters(num_sms) * kTailCluster * (size_t)S.tail_gbytes[c];
+    return b;
+}
+
+size_t tail_bytes(const UnitSet &S)
+{
+    size_t b = al16(sizeof(TailList) * kTailClasses);
+    for (int c = 0; c < kTailClasses; c++) b += al16(sizeof(TailEntry) * (size_t)std::max(S.tail_cap[c], 1));
+    return b;
+}
+
+eg_status tail_upload(const UnitSet &S, void *block, cudaStream_t st, TailList **lists)
+{
+    TailList hl[kTailClasses];
+    char *p = (char *)block;
+    char *q = p + al16(sizeof(TailList) * kTailClasses);
+    cudaError_t e = cudaSuccess;
+    for (int c = 0; c < kTailClasses; c++) {
+        hl[c].count = hl[c].init = (int)S.tail_init[c].size();
+        hl[c].next = 0;
+        hl[c].cap = S.tail_cap[c];
+        hl[c].e = (TailEntry *)q;
+        if (e == cudaSuccess && !S.tail_init[c].empty())
+            e = cudaMemcpyAsync(q, S.tail_init[c].data(), sizeof(TailEntry) * S.tail_init[c].size(),
+                                cudaMemcpyHostToDevice, st);
+        q += al16(sizeof(TailEntry) * (size_t)std::max(S.tail_cap[c], 1));
+    }
+    if (e == cudaSuccess) e = cudaMemcpyAsync(p, hl, sizeof hl, cudaMemcpyHostToDevice, st);
+    if (e != cudaSuccess) return eg_set_error(EG_ERR_CUDA, "tail list upload failed: %s", cudaGetErrorString(e));
+    *lists = (TailList *)p;
+    return EG_OK;
+}
+
 eg_status UnitLauncher::init()
 {
-    if (cudaEventCreateWithFlags(&fork, cudaEventDisableTiming) != cudaSuccess)
+    if (cudaEventCreateWithFlags(&fork, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&fork2, cudaEventDisableTiming) != cudaSuccess)
         return eg_set_error(EG_ERR_CUDA, "event creation failed");
-    for (int v = 0; v < kNumVariants; v++) {
-        if (!kernel_of(v)) continue;
+    for (int v = 0; v < kNumCtrl; v++) {
+        if (v < kNumVariants && !kernel_of(v)) continue;
         if (cudaStreamCreateWithFlags(&aux[v], cudaStreamNonBlocking) != cudaSuccess ||
             cudaEventCreateWithFlags(&join[v], cudaEventDisableTiming) != cudaSuccess)
             return eg_set_error(EG_ERR_CUDA, "stream creation failed");
@@ -617,66 +1036,148 @@ eg_status UnitLauncher::init()
 
 void UnitLauncher::destroy()
 {
-    for (int v = 0; v < kNumVariants; v++) {
+    for (int v = 0; v < kNumCtrl; v++) {
         if (aux[v]) cudaStreamDestroy(aux[v]);
         if (join[v]) cudaEventDestroy(join[v]);
         aux[v] = nullptr;
         join[v] = nullptr;
     }
     if (fork) cudaEventDestroy(fork);
-    fork = nullptr;
+    if (fork2) cudaEventDestroy(fork2);
+    fork = fork2 = nullptr;
+}
+
+/* Clusters of the tail kernel of class cls that fit the GPU at once. */
+static eg_status tail_clusters(int cls, int block, int smem, int *clusters)
+{
+    cudaLaunchConfig_t cfg;
+    memset(&cfg, 0, sizeof cfg);
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = kTailCluster;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.gridDim = dim3(kTailCluster);
+    cfg.blockDim = dim3(block);
+    cfg.dynamicSmemBytes = (size_t)smem;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    int n = 0;
+    cudaError_t e = cudaOccupancyMaxActiveClusters(&n, (const void *)tail_kernel_of(cls), &cfg);
+    if (e != cudaSuccess || n < 1)
+        return eg_set_error(EG_ERR_CUDA, "tail kernel clusters do not fit (%d B shared): %s", smem, cudaGetErrorString(e));
+    *clusters = n;
+    return EG_OK;
 }
 
 eg_status launch_unit_set(UnitLauncher &L, cudaStream_t main, const UnitSet &S, const UnitDesc *units_dev,
-                          UnitCtrl *ctrl_dev, int block, int num_sms, long long max_rounds,
-                          unsigned long long timeout_ns, int *grid_total)
+                          TailList *tails, void *tail_scratch, LaunchCtrl *ctrl, int block, int num_sms,
+                          long long max_rounds, unsigned long long timeout_ns, int *grid_total)
 {
-    cudaError_t e = cudaMemsetAsync(ctrl_dev, 0, sizeof(UnitCtrl) * kNumVariants, main);
-    if (e == cudaSuccess) e = cudaEventRecord(L.fork, main);
+    cudaError_t e = cudaMemsetAsync(ctrl, 0, sizeof(LaunchCtrl), main);
     if (e != cudaSuccess) return eg_set_error(EG_ERR_CUDA, "launch set-up failed: %s", cudaGetErrorString(e));
-    /* the variant holding the heaviest unit is launched first */
+    k_tail_rewind<<<1, 256, 0, main>>>(tails, units_dev);
+    e = cudaEventRecord(L.fork, main);
+    if (e != cudaSuccess) return eg_set_error(EG_ERR_CUDA, "launch set-up failed: %s", cudaGetErrorString(e));
+    /* phase 1: the variant holding the heaviest unit is launched first */
     std::vector<int> vs;
     for (int v = 0; v < kNumVariants; v++)
         if (S.off[v + 1] > S.off[v]) vs.push_back(v);
     std::stable_sort(vs.begin(), vs.end(), [&](int a, int c) { return S.top_cost[a] > S.top_cost[c]; });
+    std::vector<int> grids(vs.size());
     int total = 0;
-    for (int v : vs) {
+    for (size_t i = 0; i < vs.size(); i++) {
+        const int v = vs[i];
         unit_kernel_t k = kernel_of(v);
         if (!k) return eg_set_error(EG_ERR_INVALID, "no kernel for unit variant %d", v);
         int per_sm = 0;
         e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void *)k, block, (size_t)S.smem[v]);
         if (e != cudaSuccess || per_sm < 1)
             return eg_set_error(EG_ERR_CUDA, "unit kernel does not fit (block %d, %d B shared)", block, S.smem[v]);
-        const int count = S.off[v + 1] - S.off[v];
-        const int grid = std::max(1, std::min(num_sms * per_sm, count));
+        grids[i] = std::max(1, std::min(num_sms * per_sm, S.off[v + 1] - S.off[v]));
+        total += grids[i];
+    }
+    for (size_t i = 0; i < vs.size(); i++) {
+        const int v = vs[i];
         UnitParams p;
         memset(&p, 0, sizeof p);
         p.units = units_dev + S.off[v];
-        p.ctrl = ctrl_dev + v;
-        p.num_units = count;
+        p.ctrl = &ctrl->c[v];
+        p.tails = tails;
+        p.idle = &ctrl->idle;
+        p.num_units = S.off[v + 1] - S.off[v];
+        p.unit_base = S.off[v];
+        p.park_total = total;
+        p.t_start = &ctrl->t_start;
         p.max_rounds = max_rounds;
         p.timeout_ns = timeout_ns;
         void *args[] = {(void *)&p};
         e = cudaStreamWaitEvent(L.aux[v], L.fork, 0);
-        if (e == cudaSuccess) e = cudaLaunchKernel((const void *)k, dim3(grid), dim3(block), args, (size_t)S.smem[v], L.aux[v]);
+        if (e == cudaSuccess)
+            e = cudaLaunchKernel((const void *)kernel_of(v), dim3(grids[i]), dim3(block), args, (size_t)S.smem[v], L.aux[v]);
         if (e == cudaSuccess) e = cudaEventRecord(L.join[v], L.aux[v]);
         if (e == cudaSuccess) e = cudaStreamWaitEvent(main, L.join[v], 0);
         if (e != cudaSuccess) return eg_set_error(EG_ERR_CUDA, "unit kernel launch failed: %s", cudaGetErrorString(e));
-        total += grid;
+    }
+    /* phase 2: the tail lists on clusters, one kernel per class that can
+     * hold entries (those with no entries at run time exit at once) */
+    e = cudaEventRecord(L.fork2, main);
+    if (e != cudaSuccess) return eg_set_error(EG_ERR_CUDA, "launch set-up failed: %s", cudaGetErrorString(e));
+    char *gs = (char *)tail_scratch;
+    for (int c = 0; c < kTailClasses; c++) {
+        if (S.tail_cap[c] == 0) continue;
+        const int slot = kNumVariants + c;
+        int ncl = 0;
+        EG_TRY(tail_clusters(c, 1024, S.tail_smem[c], &ncl));
+        TailParams tp;
+        memset(&tp, 0, sizeof tp);
+        tp.units = units_dev;
+        tp.list = tails + c;
+        tp.ctrl = &ctrl->c[slot];
+        tp.t_start = &ctrl->t_start;
+        tp.max_rounds = max_rounds;
+        tp.timeout_ns = timeout_ns;
+        if (S.tail_gbytes[c] > 0) {
+            if (!gs) return eg_set_error(EG_ERR_INVALID, "hybrid tail without scratch");
+            ncl = std::min(ncl, tail_hyb_clusters(num_sms));
+            tp.gscratch = gs;
+            tp.gstride = S.tail_gbytes[c];
+            gs += (size_t)tail_hyb_clusters(num_sms) * kTailCluster * (size_t)S.tail_gbytes[c];
+        }
+        cudaLaunchConfig_t cfg;
+        memset(&cfg, 0, sizeof cfg);
+        cudaLaunchAttribute attr[1];
+        attr[0].id = cudaLaunchAttributeClusterDimension;
+        attr[0].val.clusterDim.x = kTailCluster;
+        attr[0].val.clusterDim.y = 1;
+        attr[0].val.clusterDim.z = 1;
+        const int ent = S.tail_cap[c];
+        cfg.gridDim = dim3(kTailCluster * std::max(1, std::min(ncl, ent)));
+        cfg.blockDim = dim3(1024);
+        cfg.dynamicSmemBytes = (size_t)S.tail_smem[c];
+        cfg.stream = L.aux[slot];
+        cfg.attrs = attr;
+        cfg.numAttrs = 1;
+        e = cudaStreamWaitEvent(L.aux[slot], L.fork2, 0);
+        if (e == cudaSuccess) e = cudaLaunchKernelEx(&cfg, tail_kernel_of(c), tp);
+        if (e == cudaSuccess) e = cudaEventRecord(L.join[slot], L.aux[slot]);
+        if (e == cudaSuccess) e = cudaStreamWaitEvent(main, L.join[slot], 0);
+        if (e != cudaSuccess) return eg_set_error(EG_ERR_CUDA, "tail kernel launch failed: %s", cudaGetErrorString(e));
     }
     if (grid_total) *grid_total = total;
     return EG_OK;
 }
 
-void sum_ctrl(const UnitCtrl *c, UnitCtrl *out)
+void sum_ctrl(const LaunchCtrl &lc, UnitCtrl *out)
 {
     memset(out, 0, sizeof *out);
-    for (int v = 0; v < kNumVariants; v++) {
-        out->lifts += c[v].lifts;
-        out->edges += c[v].edges;
-        out->num_top += c[v].num_top;
-        if (c[v].t_begin && (!out->t_begin || c[v].t_begin < out->t_begin)) out->t_begin = c[v].t_begin;
-        out->t_end = std::max(out->t_end, c[v].t_end);
+    for (int v = 0; v < kNumCtrl; v++) {
+        const UnitCtrl &c = lc.c[v];
+        out->lifts += c.lifts;
+        out->edges += c.edges;
+        out->num_top += c.num_top;
+        if (c.t_begin && (!out->t_begin || c.t_begin < out->t_begin)) out->t_begin = c.t_begin;
+        out->t_end = std::max(out->t_end, c.t_end);
     }
 }
 
@@ -692,7 +1193,7 @@ struct eg_batch {
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     int num_games = 0, K = 0, d = 1;
     long long total_nodes = 0, total_edges = 0;
-    int block = 1024, kg_cap = 8, smem_budget = 0, sms = 148;
+    int block = 1024, kg_cap = 8, smem_budget = 0, sms = 148, tail_rows = 0;
     long long max_rounds = -1;
     double timeout_ms = 0;
     std::vector<HostPacked> hp;      /* host images (slots dropped after upload) */
@@ -712,7 +1213,11 @@ struct eg_batch {
     int units_cap = 0;
     void *gscratch = nullptr;
     size_t gscratch_bytes = 0;
-    UnitCtrl *ctrl = nullptr;        /* kNumVariants counters                    */
+    LaunchCtrl *ctrl = nullptr;      /* counters of a solve                      */
+    void *tails = nullptr;           /* tail lists (tail_bytes of the plan)      */
+    size_t tails_bytes = 0;
+    void *tscratch = nullptr;        /* hybrid tail regions                      */
+    size_t tscratch_bytes = 0;
     UnitLauncher launcher;
     size_t bytes = 0, unit_bytes = 0;
     bool thresholds_set = false, solved = false, use_graph = false;
@@ -753,7 +1258,7 @@ extern "C" void eg_batch_free(eg_batch *b)
     if (b->st) cudaStreamSynchronize(b->st);
     batch_drop_graph(b);
     batch_free_units(b);
-    void *ptrs[] = {b->dblock, b->F, b->p_dev, b->mg_dev, b->ctrl};
+    void *ptrs[] = {b->dblock, b->F, b->p_dev, b->mg_dev, b->ctrl, b->tails, b->tscratch};
     for (void *q : ptrs)
         if (q) cudaFree(q);
     b->launcher.destroy();
@@ -834,6 +1339,7 @@ extern "C" eg_status eg_batch_create(const eg_game *games, int32_t num_games, co
     b->total_edges = tm;
     b->block = opts->block ? opts->block : 1024;
     b->kg_cap = opts->group_max ? opts->group_max : 8;
+    b->tail_rows = opts->tail_rows > 0 ? opts->tail_rows : 0;
     b->max_rounds = opts->max_rounds;
     b->timeout_ms = opts->timeout_ms;
     b->use_graph = opts->use_graph != 0;
@@ -870,7 +1376,7 @@ extern "C" eg_status eg_batch_create(const eg_game *games, int32_t num_games, co
     if (s == EG_OK) s = balloc(b, &b->F, (size_t)b->f_off[(size_t)num_games]);
     if (s == EG_OK) s = balloc(b, &b->p_dev, (size_t)num_games * b->K);
     if (s == EG_OK) s = balloc(b, &b->mg_dev, (size_t)num_games * b->K);
-    if (s == EG_OK) s = balloc(b, &b->ctrl, (size_t)kNumVariants);
+    if (s == EG_OK) s = balloc(b, &b->ctrl, 1);
     b->pd.resize((size_t)num_games);
     for (int g = 0; g < num_games && s == EG_OK; g++)
         s = packed_upload(b->hp[(size_t)g], (char *)b->dblock + poff[(size_t)g], b->st, &b->pd[(size_t)g]);
@@ -906,7 +1412,8 @@ static eg_status batch_plan(eg_batch *b)
         const size_t before = units.size();
         EG_TRY(make_units(b->hp[(size_t)g], b->pd[(size_t)g], K, b->d, b->p_host.data() + (size_t)g * K,
                           b->mg_host.data() + (size_t)g * K, b->p_dev + (size_t)g * K, b->mg_dev + (size_t)g * K,
-                          b->F + b->f_off[(size_t)g], b->smem_budget, b->kg_cap, &units, &gneed, &cost, &smem));
+                          b->F + b->f_off[(size_t)g], b->smem_budget, b->kg_cap, &units, &gneed, &cost, &smem,
+                          b->tail_rows));
         for (size_t i = before; i < units.size(); i++) ugame.push_back(g);
     }
     std::vector<int> perm;
@@ -944,14 +1451,45 @@ static eg_status batch_plan(eg_batch *b)
         u.status = b->u_status + j;
         b->unit_game[(size_t)j] = ugame[(size_t)perm[(size_t)j]];
     }
+    const size_t tb = tail_bytes(S);
+    if (tb > b->tails_bytes) {
+        reallocated = true;
+        if (b->tails) {
+            cudaFree(b->tails);
+            b->bytes -= b->tails_bytes;
+            b->tails = nullptr;
+            b->tails_bytes = 0;
+        }
+        EG_TRY(balloc(b, (char **)&b->tails, tb));
+        b->tails_bytes = tb;
+    }
+    const size_t tsb = tail_scratch_bytes(S, b->sms);
+    if (tsb > b->tscratch_bytes) {
+        reallocated = true;
+        if (b->tscratch) {
+            cudaFree(b->tscratch);
+            b->bytes -= b->tscratch_bytes;
+            b->tscratch = nullptr;
+            b->tscratch_bytes = 0;
+        }
+        EG_TRY(balloc(b, (char **)&b->tscratch, tsb));
+        b->tscratch_bytes = tsb;
+    }
     /* a captured graph stays valid when the plan is the same (the units read
      * their thresholds and MG from device memory at run time) */
-    const bool same = !reallocated && b->set.units.size() == S.units.size() &&
-                      memcmp(b->set.off, S.off, sizeof S.off) == 0 && memcmp(b->set.smem, S.smem, sizeof S.smem) == 0 &&
-                      memcmp(b->set.units.data(), S.units.data(), sizeof(UnitDesc) * S.units.size()) == 0;
+    bool same = !reallocated && b->set.units.size() == S.units.size() &&
+                memcmp(b->set.off, S.off, sizeof S.off) == 0 && memcmp(b->set.smem, S.smem, sizeof S.smem) == 0 &&
+                memcmp(b->set.tail_cap, S.tail_cap, sizeof S.tail_cap) == 0 &&
+                memcmp(b->set.tail_smem, S.tail_smem, sizeof S.tail_smem) == 0 &&
+                memcmp(b->set.units.data(), S.units.data(), sizeof(UnitDesc) * S.units.size()) == 0;
+    for (int c = 0; c < kTailClasses && same; c++)
+        same = b->set.tail_init[c].size() == S.tail_init[c].size() &&
+               memcmp(b->set.tail_init[c].data(), S.tail_init[c].data(), sizeof(TailEntry) * S.tail_init[c].size()) == 0;
     b->set = std::move(S);
     EG_CUDA(cudaMemcpyAsync(b->units_dev, b->set.units.data(), sizeof(UnitDesc) * (size_t)nu, cudaMemcpyHostToDevice,
                             b->st));
+    TailList *tl = nullptr;
+    EG_TRY(tail_upload(b->set, b->tails, b->st, &tl));
     EG_CUDA(cudaStreamSynchronize(b->st));
     if (!same) batch_drop_graph(b);
     return EG_OK;
@@ -980,7 +1518,8 @@ extern "C" eg_status eg_batch_set_thresholds(eg_batch *b, const int32_t *p)
 static eg_status batch_enqueue(eg_batch *b, cudaStream_t st, int *grid)
 {
     const unsigned long long tns = b->timeout_ms > 0 ? (unsigned long long)(b->timeout_ms * 1e6) : 0ull;
-    return launch_unit_set(b->launcher, st, b->set, b->units_dev, b->ctrl, b->block, b->sms, b->max_rounds, tns, grid);
+    return launch_unit_set(b->launcher, st, b->set, b->units_dev, (TailList *)b->tails, b->tscratch, b->ctrl, b->block,
+                           b->sms, b->max_rounds, tns, grid);
 }
 
 extern "C" eg_status eg_batch_solve(eg_batch *b, eg_batch_stats *stats)
@@ -1020,11 +1559,11 @@ extern "C" eg_status eg_batch_solve(eg_batch *b, eg_batch_stats *stats)
         EG_TRY(batch_enqueue(b, b->st, &grid));
     }
     EG_CUDA(cudaEventRecord(b->ev1, b->st));
-    UnitCtrl cv[kNumVariants];
+    LaunchCtrl cv;
     const size_t nu = b->set.units.size();
     b->last_rounds.assign(nu, 0);
     b->last_status.assign(nu, 0);
-    EG_CUDA(cudaMemcpyAsync(cv, b->ctrl, sizeof cv, cudaMemcpyDeviceToHost, b->st));
+    EG_CUDA(cudaMemcpyAsync(&cv, b->ctrl, sizeof cv, cudaMemcpyDeviceToHost, b->st));
     EG_CUDA(cudaMemcpyAsync(b->last_rounds.data(), b->u_rounds, sizeof(long long) * nu, cudaMemcpyDeviceToHost, b->st));
     EG_CUDA(cudaMemcpyAsync(b->last_status.data(), b->u_status, sizeof(int) * nu, cudaMemcpyDeviceToHost, b->st));
     EG_CUDA(cudaStreamSynchronize(b->st));

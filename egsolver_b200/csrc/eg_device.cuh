@@ -56,6 +56,10 @@ __device__ __forceinline__ void st_release_gpu(unsigned *p, unsigned v)
 }
 __device__ __forceinline__ int ld_volatile(const int *p) { return *(volatile const int *)p; }
 __device__ __forceinline__ long long ld_volatile(const long long *p) { return *(volatile const long long *)p; }
+__device__ __forceinline__ unsigned long long ld_volatile_u64(const unsigned long long *p)
+{
+    return *(volatile const unsigned long long *)p;
+}
 
 /* Sets bit p of a frontier bitmap; returns true when this call set it.
  * The plain L2 read first filters the common case of an already-set bit. */

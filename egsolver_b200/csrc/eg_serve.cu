@@ -116,7 +116,9 @@ struct Launch {
     cudaEvent_t ev = nullptr;
     std::vector<int64_t> qids;
     UnitDesc *dunits = nullptr;
-    UnitCtrl *dctrl = nullptr;
+    LaunchCtrl *dctrl = nullptr;
+    void *dtails = nullptr;
+    void *dscratch = nullptr;   /* hybrid tail regions */
 };
 
 }  // namespace
@@ -231,9 +233,10 @@ bool reap(eg_server *s)
         }
         any = true;
         const clk::time_point now = clk::now();
-        UnitCtrl c, cv[kNumVariants];
+        UnitCtrl c;
+        LaunchCtrl cv;
         memset(&c, 0, sizeof c);
-        if (e == cudaSuccess && cudaMemcpy(cv, l.dctrl, sizeof cv, cudaMemcpyDeviceToHost) == cudaSuccess) {
+        if (e == cudaSuccess && cudaMemcpy(&cv, l.dctrl, sizeof cv, cudaMemcpyDeviceToHost) == cudaSuccess) {
             sum_ctrl(cv, &c);
             if (!s->clock0) s->clock0 = c.t_begin;
             eg_serve_span sp;
@@ -277,6 +280,8 @@ bool reap(eg_server *s)
         cudaEventDestroy(l.ev);
         cudaFreeAsync(l.dunits, s->streams[l.stream]);
         cudaFreeAsync(l.dctrl, s->streams[l.stream]);
+        cudaFreeAsync(l.dtails, s->streams[l.stream]);
+        if (l.dscratch) cudaFreeAsync(l.dscratch, s->streams[l.stream]);
         s->inflight.erase(s->inflight.begin() + (long)i);
     }
     if (any) s->cv_done.notify_all();
@@ -439,16 +444,24 @@ bool launch_ready(eg_server *s)
     cudaStream_t st = s->streams[l.stream];
     for (int64_t qid : l.qids) cudaStreamWaitEvent(st, s->queries[qid]->ready, 0);
     cudaError_t e = cudaMallocAsync((void **)&l.dunits, sizeof(UnitDesc) * S.units.size(), st);
-    if (e == cudaSuccess) e = cudaMallocAsync((void **)&l.dctrl, sizeof(UnitCtrl) * kNumVariants, st);
+    if (e == cudaSuccess) e = cudaMallocAsync((void **)&l.dctrl, sizeof(LaunchCtrl), st);
+    if (e == cudaSuccess) e = cudaMallocAsync(&l.dtails, tail_bytes(S), st);
+    const size_t tsb = tail_scratch_bytes(S, s->sms);
+    if (e == cudaSuccess && tsb) e = cudaMallocAsync(&l.dscratch, tsb, st);
     if (e == cudaSuccess)
         e = cudaMemcpyAsync(l.dunits, S.units.data(), sizeof(UnitDesc) * S.units.size(), cudaMemcpyHostToDevice, st);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&l.ev, cudaEventDisableTiming);
     eg_status ls = EG_OK;
-    if (e == cudaSuccess) {
+    TailList *tl = nullptr;
+    if (e == cudaSuccess) ls = tail_upload(S, l.dtails, st, &tl);
+    if (e == cudaSuccess && ls == EG_OK) {
         int grid = 0;
-        ls = launch_unit_set(s->launchers[(size_t)l.stream], st, S, l.dunits, l.dctrl, s->o.block, s->sms,
-                             s->o.max_rounds, 0, &grid);
+        ls = launch_unit_set(s->launchers[(size_t)l.stream], st, S, l.dunits, tl, l.dscratch, l.dctrl, s->o.block,
+                             s->sms, s->o.max_rounds, 0, &grid);
         if (ls == EG_OK) e = cudaEventRecord(l.ev, st);
+        /* the tail lists' host image is copied from pageable memory: wait for
+         * the copy before S goes out of scope */
+        if (ls == EG_OK && e == cudaSuccess) e = cudaStreamSynchronize(s->upload_stream);
     }
     if (e != cudaSuccess || ls != EG_OK) {
         cudaGetLastError();
@@ -464,6 +477,8 @@ bool launch_ready(eg_server *s)
         if (l.ev) cudaEventDestroy(l.ev);
         if (l.dunits) cudaFreeAsync(l.dunits, st);
         if (l.dctrl) cudaFreeAsync(l.dctrl, st);
+        if (l.dtails) cudaFreeAsync(l.dtails, st);
+        if (l.dscratch) cudaFreeAsync(l.dscratch, st);
         s->ready.clear();
         s->cv_done.notify_all();
         return true;

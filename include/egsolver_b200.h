@@ -289,7 +289,10 @@ typedef struct eg_batch_opts {
                                     CUDA graph on the first solve and replayed      */
     int32_t group_max;           /* most thresholds per work unit: 1, 2, 4 or 8
                                     (0: 8; eg_batch_tune picks one)                 */
-    int32_t reserved[6];
+    int32_t tail_rows;           /* games of at least this many vertices go straight
+                                    to the cluster tail (0: only those too large
+                                    for one CTA's shared memory)                    */
+    int32_t reserved[5];
 } eg_batch_opts;
 
 typedef struct eg_batch_stats {

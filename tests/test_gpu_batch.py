@@ -83,13 +83,14 @@ def test_autotuner_then_solve():
 def test_unit_variants_match_the_oracle():
     """Every kind of work unit: 32- and 64-bit credits, 4- and 8-byte slots,
     groups of 8/4/2/1 thresholds (K = 15 splits into 8 + 4 + 2 + 1), and
-    credits in global scratch for a game too large for shared memory."""
+    hybrid credits (shared memory plus global scratch) for a game too large
+    for one CTA's shared memory."""
     rng = np.random.default_rng(21)
     games = [
         eg.generate(4, 900, 9, 60, 301, param=2),        # narrow slots, 32-bit credits
         eg.generate(4, 700, 6, 20000, 302, param=2),     # |w| > 32766 -> 8-byte slots
         eg.generate(1, 600, 3, 3, 303),                  # tiny weights, big thresholds -> 64-bit credits
-        eg.generate(4, 66000, 3, 5, 304, param=2),       # > 65534 rows -> 8-byte slots, global credits
+        eg.generate(4, 66000, 3, 5, 304, param=2),       # > 65534 rows: 8-byte slots; hybrid credits
     ]
     d = 3
     K = 15
@@ -97,12 +98,14 @@ def test_unit_variants_match_the_oracle():
     p[0] = rng.integers(-150, 151, K)
     p[1] = rng.integers(-40000, 40001, K)
     p[2] = rng.integers(-(1 << 29), 1 << 29, K)         # MG far above 2^30 for positive p
-    p[3] = rng.integers(-12, 13, K)
+    p[3] = rng.integers(-14, -2, K)                     # short climbs: the test stays quick
     with eg.Batch(games, thresholds=K, scale=d) as b:
         b.set_thresholds(p)
         _, st = b.solve()
         assert st.games_failed == 0
-        assert st.num_units >= 4 * 4
+        # 8+4+2+1 groups per small game; the large one (credits beyond one
+        # CTA's shared memory) as 15 hybrid units of one threshold
+        assert st.num_units == 3 * 4 + 15
         for g, game in enumerate(games):
             got = b.credits(g)
             for k in range(K):
