@@ -606,7 +606,7 @@ extern "C" eg_status eg_dgame_solve(eg_dgame *g, const eg_opts *opts_in, eg_stat
     if (kinds) {
         /* one slice of the pair stream per warp of the dense grid */
         p.dense_depth = opts->dense_depth == 1 ? 1 : 2;
-        p.dense_sweeps = opts->dense_sweeps ? opts->dense_sweeps : 2;
+        p.dense_sweeps = opts->dense_sweeps ? opts->dense_sweeps : kMaxDenseSweeps;
         EG_TRY(dense_grid(bits, p.dense_depth, opts->grid_ctas, &dgrid));
         const long long warps = (long long)dgrid * 16;
         const long long per = (g->npairs + warps - 1) / warps;
@@ -969,7 +969,7 @@ extern "C" eg_status eg_dgame_tune(eg_dgame *g, const eg_opts *base_in, int64_t 
     /* the defaults spelled out, so that a knob's default is not timed twice */
     if (cur.large_min_deg <= 1) cur.large_min_deg = 17;
     if (cur.task_edges <= 0) cur.task_edges = 2 * kTaskPairs;
-    if (cur.dense_sweeps <= 0) cur.dense_sweeps = 2;
+    if (cur.dense_sweeps <= 0) cur.dense_sweeps = kMaxDenseSweeps;
     if (cur.dense_depth <= 0) cur.dense_depth = 2;
     double best = 0.0;
     EG_TRY(rate_of(cur, &best));

@@ -909,6 +909,10 @@ eg_status unit_kernel_setup(int device)
         cudaError_t e = cudaFuncSetAttribute((const void *)tail_kernel_of(c), cudaFuncAttributeMaxDynamicSharedMemorySize,
                                              budget);
         if (e != cudaSuccess) return eg_set_error(EG_ERR_CUDA, "cudaFuncSetAttribute failed: %s", cudaGetErrorString(e));
+        /* 16-CTA clusters are beyond the portable 8 */
+        if (cudaFuncSetAttribute((const void *)tail_kernel_of(c), cudaFuncAttributeNonPortableClusterSizeAllowed, 1) !=
+            cudaSuccess)
+            cudaGetLastError();
     }
     return EG_OK;
 }
@@ -979,15 +983,15 @@ void group_units(const std::vector<UnitDesc> &units, const std::vector<long long
 
 static size_t al16(size_t x) { return (x + 15) & ~(size_t)15; }
 
-/* Clusters a hybrid tail class launches (its scratch holds that many). */
-static int tail_hyb_clusters(int num_sms) { return num_sms / kTailCluster + 1; }
+/* Cluster CTAs a hybrid tail class may launch: its scratch holds one
+ * region per CTA. */
+static int tail_hyb_ctas(int num_sms) { return num_sms + kTailCluster; }
 
 size_t tail_scratch_bytes(const UnitSet &S, int num_sms)
 {
     size_t b = 0;
     for (int c = 0; c < kTailClasses; c++)
-        if (S.tail_cap[c] > 0 && S.tail_gbytes[c] > 0)
-            b += (size_t)tail_hyb_clusters(num_sms) * kTailCluster * (size_t)S.tail_gbytes[c];
+        if (S.tail_cap[c] > 0 && S.tail_gbytes[c] > 0) b += (size_t)tail_hyb_ctas(num_sms) * (size_t)S.tail_gbytes[c];
     return b;
 }
 
@@ -1047,27 +1051,28 @@ void UnitLauncher::destroy()
     fork = fork2 = nullptr;
 }
 
-/* Clusters of the tail kernel of class cls that fit the GPU at once. */
-static eg_status tail_clusters(int cls, int block, int smem, int *clusters)
+/* Clusters of `csize` CTAs of the tail kernel of class cls that fit the
+ * GPU at once (0 when none). */
+static int tail_clusters(int cls, int csize, int block, int smem)
 {
     cudaLaunchConfig_t cfg;
     memset(&cfg, 0, sizeof cfg);
     cudaLaunchAttribute attr[1];
     attr[0].id = cudaLaunchAttributeClusterDimension;
-    attr[0].val.clusterDim.x = kTailCluster;
+    attr[0].val.clusterDim.x = csize;
     attr[0].val.clusterDim.y = 1;
     attr[0].val.clusterDim.z = 1;
-    cfg.gridDim = dim3(kTailCluster);
+    cfg.gridDim = dim3(csize);
     cfg.blockDim = dim3(block);
     cfg.dynamicSmemBytes = (size_t)smem;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
     int n = 0;
-    cudaError_t e = cudaOccupancyMaxActiveClusters(&n, (const void *)tail_kernel_of(cls), &cfg);
-    if (e != cudaSuccess || n < 1)
-        return eg_set_error(EG_ERR_CUDA, "tail kernel clusters do not fit (%d B shared): %s", smem, cudaGetErrorString(e));
-    *clusters = n;
-    return EG_OK;
+    if (cudaOccupancyMaxActiveClusters(&n, (const void *)tail_kernel_of(cls), &cfg) != cudaSuccess) {
+        cudaGetLastError();
+        return 0;
+    }
+    return n;
 }
 
 eg_status launch_unit_set(UnitLauncher &L, cudaStream_t main, const UnitSet &S, const UnitDesc *units_dev,
@@ -1127,8 +1132,14 @@ eg_status launch_unit_set(UnitLauncher &L, cudaStream_t main, const UnitSet &S, 
     for (int c = 0; c < kTailClasses; c++) {
         if (S.tail_cap[c] == 0) continue;
         const int slot = kNumVariants + c;
-        int ncl = 0;
-        EG_TRY(tail_clusters(c, 1024, S.tail_smem[c], &ncl));
+        /* 16-CTA clusters where they can be scheduled, else 8 */
+        int csize = kTailCluster;
+        int ncl = tail_clusters(c, csize, 1024, S.tail_smem[c]);
+        if (ncl < 1) {
+            csize = 8;
+            ncl = tail_clusters(c, csize, 1024, S.tail_smem[c]);
+        }
+        if (ncl < 1) return eg_set_error(EG_ERR_CUDA, "tail kernel clusters do not fit (%d B shared)", S.tail_smem[c]);
         TailParams tp;
         memset(&tp, 0, sizeof tp);
         tp.units = units_dev;
@@ -1139,20 +1150,20 @@ eg_status launch_unit_set(UnitLauncher &L, cudaStream_t main, const UnitSet &S, 
         tp.timeout_ns = timeout_ns;
         if (S.tail_gbytes[c] > 0) {
             if (!gs) return eg_set_error(EG_ERR_INVALID, "hybrid tail without scratch");
-            ncl = std::min(ncl, tail_hyb_clusters(num_sms));
+            ncl = std::min(ncl, tail_hyb_ctas(num_sms) / csize);
             tp.gscratch = gs;
             tp.gstride = S.tail_gbytes[c];
-            gs += (size_t)tail_hyb_clusters(num_sms) * kTailCluster * (size_t)S.tail_gbytes[c];
+            gs += (size_t)tail_hyb_ctas(num_sms) * (size_t)S.tail_gbytes[c];
         }
         cudaLaunchConfig_t cfg;
         memset(&cfg, 0, sizeof cfg);
         cudaLaunchAttribute attr[1];
         attr[0].id = cudaLaunchAttributeClusterDimension;
-        attr[0].val.clusterDim.x = kTailCluster;
+        attr[0].val.clusterDim.x = csize;
         attr[0].val.clusterDim.y = 1;
         attr[0].val.clusterDim.z = 1;
         const int ent = S.tail_cap[c];
-        cfg.gridDim = dim3(kTailCluster * std::max(1, std::min(ncl, ent)));
+        cfg.gridDim = dim3(csize * std::max(1, std::min(ncl, ent)));
         cfg.blockDim = dim3(1024);
         cfg.dynamicSmemBytes = (size_t)S.tail_smem[c];
         cfg.stream = L.aux[slot];

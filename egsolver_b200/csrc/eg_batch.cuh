@@ -112,7 +112,7 @@ struct UnitCtrl {
  * a hybrid unit keeps rows >= srows in global memory (each cluster CTA its
  * own copy there) */
 constexpr int kTailClasses = 8;
-constexpr int kTailCluster = 8; /* CTAs per cluster                                */
+constexpr int kTailCluster = 16; /* CTAs per cluster (8 where 16 cannot be scheduled) */
 struct TailEntry {
     int unit;                  /* index into the unit array                   */
     int k;                     /* threshold                                   */

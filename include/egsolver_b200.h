@@ -133,7 +133,7 @@ typedef struct eg_opts {
     int32_t dense_depth;         /* chunks in flight per warp in dense rounds: 1 (three
                                     CTAs per SM) or 2 (two CTAs per SM); 0: 2         */
     int32_t dense_sweeps;        /* sweeps of the edge stream per grid barrier in dense
-                                    rounds: 1 to 4; 0: 2                              */
+                                    rounds: 1 to 4; 0: 4                              */
 } eg_opts;
 
 typedef struct eg_stats {

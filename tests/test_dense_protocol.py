@@ -93,16 +93,3 @@ def test_every_vertex_is_finalized_once_with_its_minimum():
         slice_ = max(32, -(-per // 32) * 32)  # as eg_dgame_solve sizes it
         assert walk(P, val, slice_, nwarps + 3) == want, trial
 
-
-def test_tail_row_owner_is_exact_division():
-    """The cluster tail kernel finds the CTA holding row x as
-    (x * ceil(2^40 / R)) >> 40 with R = ceil(rows / 8) rounded up to 32; this
-    equals x // R for every row of every game the batched paths take."""
-    x = np.arange(0, (1 << 19) + 4096, dtype=np.uint64)
-    for rows in (34, 1000, 4098, 65602, 131138, (1 << 19) + 66):
-        R = ((rows + 7) // 8 + 31) & ~31
-        magic = ((1 << 40) + R - 1) // R
-        xs = x[:rows]
-        owner = (xs * np.uint64(magic)) >> np.uint64(40)
-        np.testing.assert_array_equal(owner, xs // np.uint64(R))
-        assert int(owner[-1]) < 8
