@@ -90,6 +90,10 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--variant", type=int, default=0)
     ap.add_argument("--narrow", action="store_true", help="allow 32-bit device credits where exact")
+    ap.add_argument("--case", choices=["frontier-sparse60", "units-small24", "tail-game26"], default=None,
+                    help="profiling case: one small, fixed launch of a kernel for ncu (prints a labelled line, "
+                         "not a benchmark)")
+    ap.add_argument("--case-rounds", type=int, default=3000, help="sweeps of the tail-game26 case")
     ap.add_argument("--max-rounds", type=int, default=-1,
                     help="profiling aid: cap every solve at this many rounds (the line is then not a benchmark)")
     return ap.parse_args()
@@ -540,8 +544,47 @@ def run_served(args):
     print(json.dumps(line), flush=True)
 
 
+def run_case(args):
+    """Small fixed launches for kernel profiles (ncu).  Each prints one JSON
+    line labelled "profiling_case"; none is a benchmark number."""
+    import egsolver_b200 as eg
+    from egsolver_b200 import workloads
+
+    out = {"profiling_case": args.case}
+    if args.case == "frontier-sparse60":
+        # one launch of the frontier kernel: 60 sparse rounds on the cfg2 shape at n = 2^18
+        r = eg.ResidentGame(workloads.cfg2(1 << 18))
+        st, s = r.solve(direction=eg.DIRECTION_SPARSE, max_rounds=60, raise_on_error=False)
+        out.update(rounds=s.rounds, lift_ms=s.lift_ms, edges=s.edges, lifts=s.lifts, changes=s.changes,
+                   pushes=s.pushes, grid=s.grid, block=s.block)
+        r.free()
+    elif args.case == "units-small24":
+        # phase 1 of a batch of the 24 first cfg4 games with n <= 6000, 8 thresholds, 300 sweeps
+        gs = workloads.cfg4_games(64)
+        p, d = workloads.cfg4_thresholds(64)
+        small = [i for i in range(64) if gs[i].num_nodes <= 6000][:24]
+        with eg.Batch([gs[i] for i in small], thresholds=8, scale=d, max_rounds=300) as b:
+            b.set_thresholds(p[small])
+            st, s = b.solve(raise_on_error=False)
+            out.update(ms=s.solve_ms, edges=s.edges, units=s.num_units, smem=s.smem_bytes)
+    else:
+        # one (game, threshold) on the cluster tail: cfg4 game 26 (n = 32,472) at its highest threshold
+        gs = workloads.cfg4_games(64)
+        p, d = workloads.cfg4_thresholds(64)
+        k = int(np.argmax(p[26]))
+        with eg.Batch([gs[26]], thresholds=1, scale=d, max_rounds=args.case_rounds, tail_rows=1) as b:
+            b.set_thresholds(p[26:27, k:k + 1])
+            st, s = b.solve(raise_on_error=False)
+            out.update(ms=s.solve_ms, sweeps=s.rounds_max, us_per_sweep=1e3 * s.solve_ms / max(1, s.rounds_max),
+                       tail_ms=s.tail_ms)
+    print(json.dumps(out), flush=True)
+
+
 def main():
     args = parse()
+    if args.case:
+        run_case(args)
+        return
     if args.impl == "reference":
         run_reference(args)
         return

@@ -127,7 +127,8 @@ class EgBatchOpts(C.Structure):
         ("use_graph", C.c_int32),
         ("group_max", C.c_int32),
         ("tail_rows", C.c_int32),
-        ("reserved", C.c_int32 * 5),
+        ("park_percent", C.c_int32),
+        ("reserved", C.c_int32 * 4),
     ]
 
 
@@ -149,7 +150,10 @@ class EgBatchStats(C.Structure):
         ("graph_replayed", C.c_int32),
         ("num_units", C.c_int32),
         ("smem_bytes", C.c_int32),
-        ("reserved", C.c_int32 * 2),
+        ("tail_entries", C.c_int32),
+        ("reserved", C.c_int32 * 1),
+        ("phase1_ms", C.c_double),
+        ("tail_ms", C.c_double),
     ]
 
     def as_dict(self) -> dict:

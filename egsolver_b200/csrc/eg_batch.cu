@@ -140,7 +140,6 @@ __device__ __forceinline__ void column_walk(const void *E, int i0, int W, const 
     using S = Slot<WIDE>;
     using ST = typename S::T;
     using R = Row<KG, CT>;
-    constexpr int LK = Log2<KG>::v;
 #pragma unroll
     for (int k = 0; k < KG; k++) acc[k] = MAXV ? Lim<CT>::lo_acc : Lim<CT>::hi_acc;
     for (int c = 0; c < W; c += UNR) {
@@ -245,7 +244,7 @@ __device__ __forceinline__ void run_unit(const UnitDesc &u, int uglobal, unsigne
              * CTAs have nothing left, so the GPU is running the tail; the
              * unit's open thresholds continue on clusters */
             if (P.tails && (r & 15) == 15 && ld_volatile(&P.ctrl->next) >= P.num_units &&
-                2 * ld_volatile(P.idle) >= P.park_total)
+                100 * ld_volatile(P.idle) >= P.park_percent * P.park_total)
                 atomicOr(&sh.raise[slot], 1u << 17);
         }
         __syncthreads();
@@ -390,14 +389,15 @@ namespace cg = cooperative_groups;
  * its shared memory and lifts the slices of its own row range [rank * R,
  * (rank + 1) * R) (R = ceil(rows / cluster size) rounded up to 32, so a
  * slice never straddles two ranges), gathering successor credits from its
- * local replica.  At the end of a sweep a CTA that raised a credit pushes
- * its own range into every peer's replica (16-byte stores through the
- * cluster's distributed shared memory), and a cluster barrier makes those
- * writes visible before the next sweep.  A CTA thus reads its peers'
- * credits as of the previous sweep's end: values below the least fixed
- * point, so the iteration stays a fair chaotic one; a sweep in which no CTA
- * raised anything leaves all replicas equal and every vertex lifted against
- * them, i.e. the least fixed point.  The OR of the CTAs' raise flags is
+ * local replica.  A warp that raised a credit of its slice writes the
+ * slice's 32 credits into every peer's replica right away (one coalesced
+ * store per peer through the cluster's distributed shared memory), and the
+ * cluster barrier at the end of a sweep makes every such write visible
+ * before the next sweep.  A CTA thus reads its peers' credits as of the
+ * previous sweep's end or later: values below the least fixed point, so the
+ * iteration stays a fair chaotic one; a sweep in which no CTA raised
+ * anything leaves all replicas equal and every vertex lifted against them,
+ * i.e. the least fixed point.  The OR of the CTAs' raise flags is
  * gathered in rank 0's shared memory (three rotating words, as in phase 1).
  * Random 4-byte gathers through distributed shared memory are about ten
  * times slower than local ones, hence the replicas. */
@@ -408,7 +408,6 @@ __global__ void __launch_bounds__(1024, 1) k_tail(const __grid_constant__ TailPa
     using ST = typename S::T;
     constexpr CT TOPI = Lim<CT>::top, LOWI = Lim<CT>::low;
     constexpr int UNR = sizeof(CT) == 4 ? 8 : 4;
-    constexpr int VEC = 16 / (int)sizeof(CT); /* credits per 16-byte store */
     extern __shared__ __align__(16) unsigned char smem_raw[];
     CT *F = (CT *)smem_raw;
     __shared__ int s_entry;
@@ -500,37 +499,30 @@ __global__ void __launch_bounds__(1024, 1) k_tail(const __grid_constant__ TailPa
                 }
                 const int v = 32 * s + lane;
                 const bool real = own1 ? (v - 32 * u.s0 < u.n1) : (v < u.n0);
+                bool up = false;
+                CT nv = 0;
                 if (real) {
                     const CT val = acc + pk;
-                    const CT nv = val > mgk ? TOPI : (val > 0 ? val : (CT)0);
+                    nv = val > mgk ? TOPI : (val > 0 ? val : (CT)0);
                     if (nv > ld(v)) {
                         stv(v, nv);
-                        raised = 1u;
+                        up = true;
+                    }
+                }
+                /* the slice's raised credits go to every peer's replica at
+                 * once (32 consecutive rows: one coalesced store per peer) */
+                if (__any_sync(0xffffffffu, up)) {
+                    raised = 1u;
+                    const CT x = ld(v);
+                    for (int q = 1; q < C; q++) {
+                        const int peer = (rank + q) % C;
+                        if (!HYB || v < SR) *cl.map_shared_rank(F + v, peer) = x;
+                        else __stcg((CT *)(T.gscratch + (long long)(blockIdx.x - rank + peer) * T.gstride) + (v - SR), x);
                     }
                 }
             }
             const int slot = (int)(r % 3);
-            const int any = __syncthreads_or((int)raised);
-            if (any) {
-                /* push the own range into every peer's replica: the part in
-                 * shared memory through distributed shared memory, the part
-                 * in global memory into the peer's region */
-                const int mid = max(lo, min(hi, SR));
-                const int nsv = (mid - lo) / VEC, ngv = (hi - mid) / VEC;
-                const int4 *ssrc = (const int4 *)(F + lo);
-                const int4 *gsrc = HYB ? (const int4 *)(G + (mid - SR)) : nullptr;
-                for (int q = 1; q < C; q++) {
-                    const int peer = (rank + q) % C;
-                    int4 *sdst = (int4 *)cl.map_shared_rank(F + lo, peer);
-                    for (int i = tid; i < nsv; i += blockDim.x) sdst[i] = ssrc[i];
-                    if (HYB && ngv > 0) {
-                        int4 *gdst = (int4 *)(T.gscratch + (long long)(blockIdx.x - rank + peer) * T.gstride) +
-                                     (mid - SR) / VEC;
-                        for (int i = tid; i < ngv; i += blockDim.x) __stcg(gdst + i, __ldcg(gsrc + i));
-                    }
-                }
-                if (tid == 0) atomicOr(cl.map_shared_rank(&s_word[slot], 0), 1u);
-            }
+            if (__syncthreads_or((int)raised) && tid == 0) atomicOr(cl.map_shared_rank(&s_word[slot], 0), 1u);
             if (rank == 0 && tid == 0 && T.timeout_ns && globaltimer_ns() - t0 > T.timeout_ns)
                 atomicOr(&s_word[slot], 1u << 16);
             cl.sync();
@@ -1077,7 +1069,7 @@ static int tail_clusters(int cls, int csize, int block, int smem)
 
 eg_status launch_unit_set(UnitLauncher &L, cudaStream_t main, const UnitSet &S, const UnitDesc *units_dev,
                           TailList *tails, void *tail_scratch, LaunchCtrl *ctrl, int block, int num_sms,
-                          long long max_rounds, unsigned long long timeout_ns, int *grid_total)
+                          long long max_rounds, unsigned long long timeout_ns, int *grid_total, int park_percent)
 {
     cudaError_t e = cudaMemsetAsync(ctrl, 0, sizeof(LaunchCtrl), main);
     if (e != cudaSuccess) return eg_set_error(EG_ERR_CUDA, "launch set-up failed: %s", cudaGetErrorString(e));
@@ -1113,6 +1105,8 @@ eg_status launch_unit_set(UnitLauncher &L, cudaStream_t main, const UnitSet &S, 
         p.num_units = S.off[v + 1] - S.off[v];
         p.unit_base = S.off[v];
         p.park_total = total;
+        p.park_percent = park_percent;
+        if (park_percent > 100) p.tails = nullptr; /* no parking */
         p.t_start = &ctrl->t_start;
         p.max_rounds = max_rounds;
         p.timeout_ns = timeout_ns;
@@ -1204,7 +1198,7 @@ struct eg_batch {
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     int num_games = 0, K = 0, d = 1;
     long long total_nodes = 0, total_edges = 0;
-    int block = 1024, kg_cap = 8, smem_budget = 0, sms = 148, tail_rows = 0;
+    int block = 1024, kg_cap = 8, smem_budget = 0, sms = 148, tail_rows = 0, park_percent = 20;
     long long max_rounds = -1;
     double timeout_ms = 0;
     std::vector<HostPacked> hp;      /* host images (slots dropped after upload) */
@@ -1351,6 +1345,7 @@ extern "C" eg_status eg_batch_create(const eg_game *games, int32_t num_games, co
     b->block = opts->block ? opts->block : 1024;
     b->kg_cap = opts->group_max ? opts->group_max : 8;
     b->tail_rows = opts->tail_rows > 0 ? opts->tail_rows : 0;
+    b->park_percent = opts->park_percent > 0 ? opts->park_percent : 20;
     b->max_rounds = opts->max_rounds;
     b->timeout_ms = opts->timeout_ms;
     b->use_graph = opts->use_graph != 0;
@@ -1530,7 +1525,7 @@ static eg_status batch_enqueue(eg_batch *b, cudaStream_t st, int *grid)
 {
     const unsigned long long tns = b->timeout_ms > 0 ? (unsigned long long)(b->timeout_ms * 1e6) : 0ull;
     return launch_unit_set(b->launcher, st, b->set, b->units_dev, (TailList *)b->tails, b->tscratch, b->ctrl, b->block,
-                           b->sms, b->max_rounds, tns, grid);
+                           b->sms, b->max_rounds, tns, grid, b->park_percent);
 }
 
 extern "C" eg_status eg_batch_solve(eg_batch *b, eg_batch_stats *stats)
@@ -1580,6 +1575,19 @@ extern "C" eg_status eg_batch_solve(eg_batch *b, eg_batch_stats *stats)
     EG_CUDA(cudaStreamSynchronize(b->st));
     UnitCtrl c;
     sum_ctrl(cv, &c);
+    /* the two phases on the device clock */
+    unsigned long long p1b = 0, p1e = 0, tb = 0, te = 0;
+    for (int v = 0; v < kNumCtrl; v++) {
+        const UnitCtrl &x = cv.c[v];
+        if (!x.t_begin) continue;
+        unsigned long long &b0 = v < kNumVariants ? p1b : tb, &e0 = v < kNumVariants ? p1e : te;
+        if (!b0 || x.t_begin < b0) b0 = x.t_begin;
+        e0 = std::max(e0, x.t_end);
+    }
+    TailList tls[kTailClasses];
+    EG_CUDA(cudaMemcpy(tls, b->tails, sizeof tls, cudaMemcpyDeviceToHost));
+    int tail_entries = 0;
+    for (int t = 0; t < kTailClasses; t++) tail_entries += std::min(tls[t].count, tls[t].cap);
     float ms = 0.f;
     cudaEventElapsedTime(&ms, b->ev0, b->ev1);
     b->solved = true;
@@ -1617,6 +1625,9 @@ extern "C" eg_status eg_batch_solve(eg_batch *b, eg_batch_stats *stats)
         stats->graph_replayed = replay ? 1 : 0;
         stats->num_units = (int32_t)nu;
         stats->smem_bytes = smem;
+        stats->tail_entries = tail_entries;
+        stats->phase1_ms = p1e > p1b ? (double)(p1e - p1b) * 1e-6 : 0.0;
+        stats->tail_ms = te > tb ? (double)(te - tb) * 1e-6 : 0.0;
     }
     if (first != EG_OK) return eg_set_error(first, "%d game(s) stopped early (status %d)", failed, (int)first);
     return EG_OK;

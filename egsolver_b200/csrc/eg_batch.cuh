@@ -137,7 +137,7 @@ struct UnitParams {
     int num_units;
     int unit_base;             /* index of units[0] in the whole unit array    */
     int park_total;            /* CTAs of all phase-1 kernels of the launch    */
-    int pad;
+    int park_percent;          /* park when this share of them is idle         */
     unsigned long long *t_start;   /* device clock of the launch's first CTA      */
     long long max_rounds;          /* per unit; < 0: none                        */
     unsigned long long timeout_ns; /* per launch, from t_start; 0: none          */
@@ -240,7 +240,8 @@ struct LaunchCtrl {
  * is reset and the tail lists rewound on `main` first. */
 eg_status launch_unit_set(UnitLauncher &L, cudaStream_t main, const UnitSet &S, const UnitDesc *units_dev,
                           TailList *tails, void *tail_scratch, LaunchCtrl *ctrl, int block, int num_sms,
-                          long long max_rounds, unsigned long long timeout_ns, int *grid_total);
+                          long long max_rounds, unsigned long long timeout_ns, int *grid_total,
+                          int park_percent = 20);
 /* Totals of the per-variant and per-tail-class counters. */
 void sum_ctrl(const LaunchCtrl &c, UnitCtrl *out);
 

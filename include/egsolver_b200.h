@@ -290,9 +290,11 @@ typedef struct eg_batch_opts {
     int32_t group_max;           /* most thresholds per work unit: 1, 2, 4 or 8
                                     (0: 8; eg_batch_tune picks one)                 */
     int32_t tail_rows;           /* games of at least this many vertices go straight
-                                    to the cluster tail (0: only those too large
-                                    for one CTA's shared memory)                    */
-    int32_t reserved[5];
+                                    to the cluster tail (0: none)                   */
+    int32_t park_percent;        /* running units move to the cluster tail once this
+                                    share of phase-1 CTAs is idle (0: 20; above 100:
+                                    never)                                          */
+    int32_t reserved[4];
 } eg_batch_opts;
 
 typedef struct eg_batch_stats {
@@ -306,7 +308,10 @@ typedef struct eg_batch_stats {
     int32_t block, grid, games_failed, graph_replayed;
     int32_t num_units;               /* work units (game x threshold group)           */
     int32_t smem_bytes;              /* dynamic shared memory per CTA                 */
-    int32_t reserved[2];
+    int32_t tail_entries;            /* (unit, threshold) pairs the cluster tail ran  */
+    int32_t reserved[1];
+    double  phase1_ms;               /* device clock: first to last phase-1 CTA       */
+    double  tail_ms;                 /* device clock: first to last tail CTA          */
 } eg_batch_stats;
 
 /* Packs the games (each in eg_game form; all at most 2^19 vertices) on the
