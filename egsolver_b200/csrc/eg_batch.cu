@@ -570,6 +570,53 @@ __global__ void __launch_bounds__(1024, 1) k_tail(const __grid_constant__ TailPa
     }
 }
 
+/* Heaviest first: sorts each tail list by the work its entry has shown so
+ * far (sweeps x edges; an entry listed by the host counts n / 4 sweeps), one
+ * CTA per class, bitonic over the list padded to a power of two with
+ * entries of key -1 (unit -1) that sort last. */
+__device__ __forceinline__ double tail_key(const TailEntry &e, const UnitDesc *units)
+{
+    if (e.unit < 0) return -1.0;
+    const UnitDesc &u = units[e.unit];
+    const double sw = e.resume ? (double)e.sweeps : (double)u.n * 0.25;
+    return sw * (double)u.m;
+}
+
+__global__ void k_tail_order(TailList *lists, const UnitDesc *units)
+{
+    TailList &l = lists[blockIdx.x];
+    const int n = min(l.count, l.cap);
+    if (n < 2) return;
+    int N = 1;
+    while (N < n) N <<= 1;
+    for (int i = n + threadIdx.x; i < N; i += blockDim.x) {
+        TailEntry pad;
+        pad.unit = -1;
+        pad.k = 0;
+        pad.sweeps = 0;
+        pad.resume = 0;
+        pad.pad = 0;
+        l.e[i] = pad;
+    }
+    __syncthreads();
+    for (int k = 2; k <= N; k <<= 1) {
+        for (int j = k >> 1; j > 0; j >>= 1) {
+            for (int i = threadIdx.x; i < N; i += blockDim.x) {
+                const int m = i ^ j;
+                if (m <= i) continue;
+                const TailEntry a = l.e[i], b = l.e[m];
+                const double ka = tail_key(a, units), kb = tail_key(b, units);
+                const bool desc = (i & k) == 0; /* descending runs first */
+                if (desc ? (ka < kb) : (ka > kb)) {
+                    l.e[i] = b;
+                    l.e[m] = a;
+                }
+            }
+            __syncthreads();
+        }
+    }
+}
+
 typedef void (*tail_kernel_t)(TailParams);
 
 tail_kernel_t tail_kernel_of(int cls)
@@ -594,7 +641,9 @@ __global__ void k_tail_rewind(TailList *lists, const UnitDesc *units)
     for (int c = 0; c < kTailClasses; c++) {
         const TailList &l = lists[c];
         for (int i = threadIdx.x; i < l.init; i += blockDim.x) {
-            const UnitDesc &u = units[l.e[i].unit];
+            const TailEntry en = l.ie[i];
+            l.e[i] = en; /* the previous solve's sort moved them */
+            const UnitDesc &u = units[en.unit];
             *u.rounds = 0;
             *u.status = EG_OK;
         }
@@ -987,10 +1036,19 @@ size_t tail_scratch_bytes(const UnitSet &S, int num_sms)
     return b;
 }
 
+static int pow2_ceil(int x)
+{
+    int p = 1;
+    while (p < x) p <<= 1;
+    return p;
+}
+
 size_t tail_bytes(const UnitSet &S)
 {
     size_t b = al16(sizeof(TailList) * kTailClasses);
-    for (int c = 0; c < kTailClasses; c++) b += al16(sizeof(TailEntry) * (size_t)std::max(S.tail_cap[c], 1));
+    for (int c = 0; c < kTailClasses; c++)
+        b += al16(sizeof(TailEntry) * (size_t)pow2_ceil(std::max(S.tail_cap[c], 1))) +
+             al16(sizeof(TailEntry) * std::max<size_t>(S.tail_init[c].size(), 1));
     return b;
 }
 
@@ -1004,11 +1062,15 @@ eg_status tail_upload(const UnitSet &S, void *block, cudaStream_t st, TailList *
         hl[c].count = hl[c].init = (int)S.tail_init[c].size();
         hl[c].next = 0;
         hl[c].cap = S.tail_cap[c];
+        hl[c].cap2 = pow2_ceil(std::max(S.tail_cap[c], 1));
+        hl[c].pad = 0;
         hl[c].e = (TailEntry *)q;
+        q += al16(sizeof(TailEntry) * (size_t)hl[c].cap2);
+        hl[c].ie = (const TailEntry *)q;
         if (e == cudaSuccess && !S.tail_init[c].empty())
             e = cudaMemcpyAsync(q, S.tail_init[c].data(), sizeof(TailEntry) * S.tail_init[c].size(),
                                 cudaMemcpyHostToDevice, st);
-        q += al16(sizeof(TailEntry) * (size_t)std::max(S.tail_cap[c], 1));
+        q += al16(sizeof(TailEntry) * std::max<size_t>(S.tail_init[c].size(), 1));
     }
     if (e == cudaSuccess) e = cudaMemcpyAsync(p, hl, sizeof hl, cudaMemcpyHostToDevice, st);
     if (e != cudaSuccess) return eg_set_error(EG_ERR_CUDA, "tail list upload failed: %s", cudaGetErrorString(e));
@@ -1118,8 +1180,10 @@ eg_status launch_unit_set(UnitLauncher &L, cudaStream_t main, const UnitSet &S, 
         if (e == cudaSuccess) e = cudaStreamWaitEvent(main, L.join[v], 0);
         if (e != cudaSuccess) return eg_set_error(EG_ERR_CUDA, "unit kernel launch failed: %s", cudaGetErrorString(e));
     }
-    /* phase 2: the tail lists on clusters, one kernel per class that can
-     * hold entries (those with no entries at run time exit at once) */
+    /* phase 2: the tail lists on clusters, heaviest entries first, one
+     * kernel per class that can hold entries (those with no entries at run
+     * time exit at once) */
+    k_tail_order<<<kTailClasses, 1024, 0, main>>>(tails, units_dev);
     e = cudaEventRecord(L.fork2, main);
     if (e != cudaSuccess) return eg_set_error(EG_ERR_CUDA, "launch set-up failed: %s", cudaGetErrorString(e));
     char *gs = (char *)tail_scratch;

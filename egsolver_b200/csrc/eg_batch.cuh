@@ -122,7 +122,9 @@ struct TailEntry {
 };
 struct TailList {
     int count, next, cap, init;  /* entries, taken, capacity, listed by the host */
-    TailEntry *e;
+    int cap2, pad;               /* capacity rounded up to a power of two        */
+    TailEntry *e;                /* cap2 entries                                 */
+    const TailEntry *ie;         /* the init host-listed entries, kept intact    */
 };
 __host__ __device__ inline int tail_class(int variant)
 {
