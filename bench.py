@@ -90,6 +90,8 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--variant", type=int, default=0)
     ap.add_argument("--narrow", action="store_true", help="allow 32-bit device credits where exact")
+    ap.add_argument("--tune", action="store_true",
+                    help="autotune the layout and dense-round knobs (eg_dgame_tune) before the timed steps")
     ap.add_argument("--case", choices=["frontier-sparse60", "units-small24", "tail-game26"], default=None,
                     help="profiling case: one small, fixed launch of a kernel for ncu (prints a labelled line, "
                          "not a benchmark)")
@@ -624,6 +626,13 @@ def main():
     kw = dict(credit_bits=credit_bits, device=local, variant=args.variant, max_rounds=args.max_rounds,
               narrow=args.narrow)
     capped = args.max_rounds >= 0
+    tuned = None
+    if args.tune:
+        knobs, rep = res.tune(rounds=300, **kw)
+        kw.update(knobs)
+        tuned = {"knobs": knobs, **rep}
+        progress(f"tuned: {knobs} ({rep['candidates']} capped solves, {rep['default_rate']:.0f} -> "
+                 f"{rep['best_rate']:.0f} edges/ms)")
     for _ in range(args.warmup):
         flush.fill_(1)
         torch.cuda.synchronize()
@@ -760,7 +769,7 @@ def main():
                 "scaling": "weak", "vs_baseline": None, "dtype": f"int{last.credit_bits}", "data": "synthetic",
                 "config": cfg,
                 "roofline": roofline, "cpu_baseline": cpu, "cpu_baseline_omp": cpu_omp, "e2e": e2e,
-                "time_to_solution": tts,
+                "time_to_solution": tts, "tuned": tuned,
                 "gpu_launches": int(launches),
                 "clocks": clocks,
                 "solve": {"rounds": last.rounds, "lifts": last.lifts, "edges": last.edges, "changes": last.changes,

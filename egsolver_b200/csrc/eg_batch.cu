@@ -1187,17 +1187,28 @@ eg_status launch_unit_set(UnitLauncher &L, cudaStream_t main, const UnitSet &S, 
     e = cudaEventRecord(L.fork2, main);
     if (e != cudaSuccess) return eg_set_error(EG_ERR_CUDA, "launch set-up failed: %s", cudaGetErrorString(e));
     char *gs = (char *)tail_scratch;
+    int dev = 0;
+    cudaGetDevice(&dev);
     for (int c = 0; c < kTailClasses; c++) {
         if (S.tail_cap[c] == 0) continue;
         const int slot = kNumVariants + c;
+        /* a tail CTA owns its SM: asking for more than half of an SM's
+         * shared memory keeps a second CTA (of this or another cluster) off
+         * it, which would halve a heavy entry's sweep rate */
+        int sm_smem = 0;
+        if (cudaDeviceGetAttribute(&sm_smem, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev) != cudaSuccess) {
+            cudaGetLastError();
+            sm_smem = 0;
+        }
+        const int tsmem = std::max(S.tail_smem[c], std::min(sm_smem / 2 + 1024, unit_smem_budget(dev)));
         /* 16-CTA clusters where they can be scheduled, else 8 */
         int csize = kTailCluster;
-        int ncl = tail_clusters(c, csize, 1024, S.tail_smem[c]);
+        int ncl = tail_clusters(c, csize, 1024, tsmem);
         if (ncl < 1) {
             csize = 8;
-            ncl = tail_clusters(c, csize, 1024, S.tail_smem[c]);
+            ncl = tail_clusters(c, csize, 1024, tsmem);
         }
-        if (ncl < 1) return eg_set_error(EG_ERR_CUDA, "tail kernel clusters do not fit (%d B shared)", S.tail_smem[c]);
+        if (ncl < 1) return eg_set_error(EG_ERR_CUDA, "tail kernel clusters do not fit (%d B shared)", tsmem);
         TailParams tp;
         memset(&tp, 0, sizeof tp);
         tp.units = units_dev;
@@ -1223,7 +1234,7 @@ eg_status launch_unit_set(UnitLauncher &L, cudaStream_t main, const UnitSet &S, 
         const int ent = S.tail_cap[c];
         cfg.gridDim = dim3(csize * std::max(1, std::min(ncl, ent)));
         cfg.blockDim = dim3(1024);
-        cfg.dynamicSmemBytes = (size_t)S.tail_smem[c];
+        cfg.dynamicSmemBytes = (size_t)tsmem;
         cfg.stream = L.aux[slot];
         cfg.attrs = attr;
         cfg.numAttrs = 1;
@@ -1262,7 +1273,7 @@ struct eg_batch {
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     int num_games = 0, K = 0, d = 1;
     long long total_nodes = 0, total_edges = 0;
-    int block = 1024, kg_cap = 8, smem_budget = 0, sms = 148, tail_rows = 0, park_percent = 20;
+    int block = 1024, kg_cap = 8, smem_budget = 0, sms = 148, tail_rows = 0, park_percent = 10;
     long long max_rounds = -1;
     double timeout_ms = 0;
     std::vector<HostPacked> hp;      /* host images (slots dropped after upload) */
@@ -1409,7 +1420,7 @@ extern "C" eg_status eg_batch_create(const eg_game *games, int32_t num_games, co
     b->block = opts->block ? opts->block : 1024;
     b->kg_cap = opts->group_max ? opts->group_max : 8;
     b->tail_rows = opts->tail_rows > 0 ? opts->tail_rows : 0;
-    b->park_percent = opts->park_percent > 0 ? opts->park_percent : 20;
+    b->park_percent = opts->park_percent > 0 ? opts->park_percent : 10;
     b->max_rounds = opts->max_rounds;
     b->timeout_ms = opts->timeout_ms;
     b->use_graph = opts->use_graph != 0;

@@ -243,7 +243,7 @@ struct LaunchCtrl {
 eg_status launch_unit_set(UnitLauncher &L, cudaStream_t main, const UnitSet &S, const UnitDesc *units_dev,
                           TailList *tails, void *tail_scratch, LaunchCtrl *ctrl, int block, int num_sms,
                           long long max_rounds, unsigned long long timeout_ns, int *grid_total,
-                          int park_percent = 20);
+                          int park_percent = 10);
 /* Totals of the per-variant and per-tail-class counters. */
 void sum_ctrl(const LaunchCtrl &c, UnitCtrl *out);
 

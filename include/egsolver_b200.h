@@ -292,7 +292,7 @@ typedef struct eg_batch_opts {
     int32_t tail_rows;           /* games of at least this many vertices go straight
                                     to the cluster tail (0: none)                   */
     int32_t park_percent;        /* running units move to the cluster tail once this
-                                    share of phase-1 CTAs is idle (0: 20; above 100:
+                                    share of phase-1 CTAs is idle (0: 10; above 100:
                                     never)                                          */
     int32_t reserved[4];
 } eg_batch_opts;
