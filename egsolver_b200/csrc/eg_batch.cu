@@ -1736,43 +1736,36 @@ extern "C" eg_status eg_batch_game_result(eg_batch *b, int32_t game, int64_t *ro
     return EG_OK;
 }
 
-/* Autotuner: every candidate (CTA size, largest threshold group) plans the
- * batch and solves it under a sweep cap (enough sweeps to reach the steady
- * state, few enough to be quick); the candidate with the most edge
- * relaxations per second is kept. */
+/* Autotuner: every candidate CTA size solves the planned batch under a
+ * sweep cap (enough sweeps to reach the steady state, few enough to be
+ * quick); the candidate with the most edge relaxations per second is kept.
+ * The threshold group size stays as configured: a capped solve favours one
+ * threshold per unit (more CTAs busy early), while the whole solve is faster
+ * with groups of eight (each sweep of a unit relaxes eight thresholds, and
+ * the long-running thresholds reach the cluster tail together). */
 extern "C" eg_status eg_batch_tune(eg_batch *b, int32_t *block_out)
 {
     if (!b) return eg_set_error(EG_ERR_INVALID, "batch is NULL");
     if (!b->thresholds_set) return eg_set_error(EG_ERR_INVALID, "thresholds not set");
     const int blocks[] = {512, 1024};
-    const int groups[] = {8, 4, 2, 1};
     const long long keep_cap = b->max_rounds;
     const bool keep_graph = b->use_graph;
-    const int keep_kg = b->kg_cap;
     b->use_graph = false;
     b->max_rounds = 48;
     double best = -1.0;
-    int best_block = b->block, best_kg = keep_kg;
-    for (int kg : groups) {
-        if (kg > keep_kg) continue;
-        b->kg_cap = kg;
-        eg_status ps = batch_plan(b);
-        if (ps != EG_OK) continue;
-        for (int c : blocks) {
-            b->block = c;
-            eg_batch_stats st;
-            eg_status s = eg_batch_solve(b, &st);
-            if (s != EG_OK && s != EG_ERR_LOOPCAP) continue;
-            const double rate = st.solve_ms > 0 ? (double)st.edges / st.solve_ms : 0.0;
-            if (rate > best) {
-                best = rate;
-                best_block = c;
-                best_kg = kg;
-            }
+    int best_block = b->block;
+    for (int c : blocks) {
+        b->block = c;
+        eg_batch_stats st;
+        eg_status s = eg_batch_solve(b, &st);
+        if (s != EG_OK && s != EG_ERR_LOOPCAP) continue;
+        const double rate = st.solve_ms > 0 ? (double)st.edges / st.solve_ms : 0.0;
+        if (rate > best) {
+            best = rate;
+            best_block = c;
         }
     }
     b->block = best_block;
-    b->kg_cap = best_kg;
     b->max_rounds = keep_cap;
     b->use_graph = keep_graph;
     b->solved = false;

@@ -281,14 +281,14 @@ typedef struct eg_batch eg_batch;
 typedef struct eg_batch_opts {
     int32_t thresholds;          /* K thresholds per game, 1..EG_BATCH_MAX_K        */
     int32_t scale;               /* d >= 1: threshold p turns w into w*d - p        */
-    int32_t block;               /* threads per CTA (64..1024); 0 = 1024 (eg_batch_tune picks one) */
+    int32_t block;               /* threads per CTA (64..1024); 0 = 1024 (eg_batch_tune picks 512 or 1024) */
     int32_t device;
     int64_t max_rounds;          /* per game; < 0: no cap                           */
     double  timeout_ms;          /* per launch; <= 0: none                          */
     int32_t use_graph;           /* non-zero: the solve's launches are captured in a
                                     CUDA graph on the first solve and replayed      */
     int32_t group_max;           /* most thresholds per work unit: 1, 2, 4 or 8
-                                    (0: 8; eg_batch_tune picks one)                 */
+                                    (0: 8)                                          */
     int32_t tail_rows;           /* games of at least this many vertices go straight
                                     to the cluster tail (0: none)                   */
     int32_t park_percent;        /* running units move to the cluster tail once this
@@ -327,9 +327,9 @@ eg_status eg_batch_credits(eg_batch *b, int32_t game, int64_t *credits);
 /* Per-game outcome of the last solve: sweeps (the most of its units) and an
  * eg_status. */
 eg_status eg_batch_game_result(eg_batch *b, int32_t game, int64_t *rounds, int32_t *status);
-/* Autotuner: times the candidate CTA sizes and threshold-group sizes on
- * the whole batch under a sweep cap and keeps the fastest for later solves
- * (*block receives the CTA size). */
+/* Autotuner: times the candidate CTA sizes on the whole batch under a
+ * sweep cap and keeps the fastest for later solves (*block receives the CTA
+ * size); the threshold group size stays as configured. */
 eg_status eg_batch_tune(eg_batch *b, int32_t *block);
 int64_t eg_batch_device_bytes(const eg_batch *b);
 void eg_batch_free(eg_batch *b);

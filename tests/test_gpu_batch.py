@@ -74,9 +74,10 @@ def test_autotuner_then_solve():
     with eg.Batch(games, thresholds=8, scale=3) as b:
         b.set_thresholds(p)
         blk = b.tune()
-        assert blk in (128, 256, 512, 1024)
+        assert blk in (512, 1024)
         _, st = b.solve()
         assert st.block == blk
+        assert st.num_units == len(games)     # K = 8: the group size stays at eight
         check_batch(b, games, p, 3)
 
 
@@ -148,3 +149,25 @@ def test_owner_arrays_in_a_batch():
         b.solve()
         np.testing.assert_array_equal(b.credits(0), b.credits(1))
         check_batch(b, [g], p[:1], 1)  # the oracle takes the split convention of g
+
+
+def test_cfg4_game_near_the_top_of_the_size_range():
+    """A cfg4 game of 17,931 vertices at all 8 thresholds (one of them
+    drives every credit to TOP, which runs into the cluster tail): two
+    thresholds against the oracle's worklist solve, all eight by the
+    oracle's fixed-point check."""
+    games = workloads.cfg4_games(64)
+    p_all, d = workloads.cfg4_thresholds(64)
+    g = games[34]
+    assert g.num_nodes == 17931
+    with eg.Batch([g], thresholds=8, scale=d) as b:
+        b.set_thresholds(p_all[34:35])
+        _, st = b.solve()
+        assert st.games_failed == 0
+        got = b.credits(0)
+    for k in range(8):
+        tg = eg.threshold_game(g, int(p_all[34, k]), d)
+        assert O.count_inconsistent(tg, got[k]) == 0, f"threshold {k}"
+    for k in (0, 2):
+        want, _ = O.eg_solve(eg.threshold_game(g, int(p_all[34, k]), d), bits=64)
+        np.testing.assert_array_equal(got[k], want)
