@@ -385,29 +385,119 @@ unit_kernel_t kernel_of(int v)
 
 namespace cg = cooperative_groups;
 
+/* Sweeps a CTA runs between two cluster barriers. */
+constexpr int kTailSweeps = 4;
+
 /* Every CTA of the cluster holds a full replica of the unit's credits in
  * its shared memory and lifts the slices of its own row range [rank * R,
  * (rank + 1) * R) (R = ceil(rows / cluster size) rounded up to 32, so a
  * slice never straddles two ranges), gathering successor credits from its
- * local replica.  A warp that raised a credit of its slice writes the
- * slice's 32 credits into every peer's replica right away (one coalesced
- * store per peer through the cluster's distributed shared memory), and the
- * cluster barrier at the end of a sweep makes every such write visible
- * before the next sweep.  A CTA thus reads its peers' credits as of the
- * previous sweep's end or later: values below the least fixed point, so the
- * iteration stays a fair chaotic one; a sweep in which no CTA raised
- * anything leaves all replicas equal and every vertex lifted against them,
- * i.e. the least fixed point.  The OR of the CTAs' raise flags is
+ * local replica.  The range's slots are copied into shared memory behind
+ * the replica when they fit, so a sweep touches no global memory.  A warp
+ * that raised a credit of its slice writes the slice's 32 credits into
+ * every peer's replica right away (one coalesced store per peer through
+ * the cluster's distributed shared memory).
+ *
+ * A CTA runs up to kTailSweeps sweeps between two cluster barriers, its
+ * warps without waiting for one another, and reads whatever its replica
+ * holds: every value there is a credit some CTA computed, hence below the
+ * least fixed point, so the iteration stays a fair chaotic one.  The
+ * barrier makes every write before it visible after it.  If no CTA raised
+ * anything between two barriers, nothing was written there either, so each
+ * vertex was lifted against the state of the first barrier without rising:
+ * that state is the least fixed point.  The OR of the CTAs' raise flags is
  * gathered in rank 0's shared memory (three rotating words, as in phase 1).
  * Random 4-byte gathers through distributed shared memory are about ten
  * times slower than local ones, hence the replicas. */
 template <typename CT, bool WIDE, bool HYB>
-__global__ void __launch_bounds__(1024, 1) k_tail(const __grid_constant__ TailParams T)
-{
+struct TailSweep {
     using S = Slot<WIDE>;
     using ST = typename S::T;
+    static constexpr int UNR = sizeof(CT) == 4 ? 4 : 2;
+    CT *F;             /* the replica (shared memory)                          */
+    CT *G;             /* hybrid: rows >= SR of this CTA's replica (global)    */
+    const ST *Es;      /* the range's slots in shared memory (staged) or null  */
+    const ST *Eg;      /* the unit's slots in global memory                    */
+    const int *slice_off;
+    char *gpeer0;      /* hybrid: the cluster's first global region            */
+    long long gstride;
+    int SR, s_lo, s_hi, s0, n0, n1, b0, rank, C;
+    CT pk, mgk, d;
+
+    __device__ __forceinline__ CT ld(int row) const
+    {
+        return (!HYB || row < SR) ? F[row] : (CT)__ldcg(G + (row - SR));
+    }
+
+    /* One sweep of the warp's slices; true if a credit rose.  Slots are
+     * read through a generic pointer: shared memory when staged, else
+     * global memory. */
+    __device__ __forceinline__ bool sweep(cg::cluster_group &cl, int lane, int warp, int nwarps) const
+    {
+        bool raised = false;
+        for (int s = s_lo + warp; s < s_hi; s += nwarps) {
+            const int b = __ldg(slice_off + s);
+            const int W = (__ldg(slice_off + s + 1) - b) >> 5;
+            const bool own1 = s >= s0;
+            CT acc = own1 ? Lim<CT>::lo_acc : Lim<CT>::hi_acc;
+            const ST *E = Es ? Es + (b - b0) : Eg + b;
+            for (int c = 0; c < W; c += UNR) {
+                ST q[UNR];
+#pragma unroll
+                for (int x = 0; x < UNR; x++)
+                    if (c + x < W) q[x] = E[lane + 32 * (c + x)];
+                CT f[UNR];
+                int wt[UNR];
+#pragma unroll
+                for (int x = 0; x < UNR; x++) {
+                    if (c + x < W) {
+                        int sc;
+                        S::dec(q[x], sc, wt[x]);
+                        f[x] = ld(sc);
+                    }
+                }
+#pragma unroll
+                for (int x = 0; x < UNR; x++) {
+                    if (c + x < W) {
+                        const CT y = f[x] - (CT)wt[x] * d;
+                        acc = own1 ? (y > acc ? y : acc) : (y < acc ? y : acc);
+                    }
+                }
+            }
+            const int v = 32 * s + lane;
+            const bool real = own1 ? (v - 32 * s0 < n1) : (v < n0);
+            bool up = false;
+            if (real) {
+                const CT val = acc + pk;
+                const CT nv = val > mgk ? Lim<CT>::top : (val > 0 ? val : (CT)0);
+                if (nv > ld(v)) {
+                    if (!HYB || v < SR) F[v] = nv;
+                    else __stcg(G + (v - SR), nv);
+                    up = true;
+                }
+            }
+            /* the slice's raised credits go to every peer's replica at once
+             * (32 consecutive rows: one coalesced store per peer) */
+            if (__any_sync(0xffffffffu, up)) {
+                raised = true;
+                const CT x = ld(v);
+                for (int q = 1; q < C; q++) {
+                    const int peer = rank + q < C ? rank + q : rank + q - C;
+                    if (!HYB || v < SR) *cl.map_shared_rank(F + v, peer) = x;
+                    else __stcg((CT *)(gpeer0 + (long long)peer * gstride) + (v - SR), x);
+                }
+            }
+        }
+        return raised;
+    }
+};
+
+template <typename CT, bool WIDE, bool HYB>
+__global__ void __launch_bounds__(1024, 1) k_tail(const __grid_constant__ TailParams T)
+{
+    using TS = TailSweep<CT, WIDE, HYB>;
+    using ST = typename TS::ST;
     constexpr CT TOPI = Lim<CT>::top, LOWI = Lim<CT>::low;
-    constexpr int UNR = sizeof(CT) == 4 ? 8 : 4;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     CT *F = (CT *)smem_raw;
     __shared__ int s_entry;
@@ -417,7 +507,7 @@ __global__ void __launch_bounds__(1024, 1) k_tail(const __grid_constant__ TailPa
     const int C = (int)cl.num_blocks();
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nwarps = blockDim.x >> 5;
     /* hybrid: rows >= srows of this CTA's replica live in its own global
-     * region, which its peers write at sweep ends (read through L2) */
+     * region, which its peers write (read through L2) */
     CT *G = HYB ? (CT *)(T.gscratch + (long long)blockIdx.x * T.gstride) : nullptr;
     if (tid == 0) {
         const unsigned long long now = globaltimer_ns();
@@ -434,18 +524,30 @@ __global__ void __launch_bounds__(1024, 1) k_tail(const __grid_constant__ TailPa
         cl.sync();
         if (ei >= T.list->count || ei >= T.list->cap) break;
         const TailEntry en = T.list->e[ei];
-        const UnitDesc u = T.units[en.unit];
+        const UnitDesc &u = T.units[en.unit];
         const int k = en.k;
         const int npad = 32 * u.ns, rows = npad + 2;
-        const int SR = HYB ? u.srows : rows; /* rows in shared memory */
         const int R = (((rows + C - 1) / C) + 31) & ~31;
         const int lo = min(rows, rank * R);
         const int hi = min(npad, lo + R); /* own rows */
-        auto ld = [&](int row) -> CT { return (!HYB || row < SR) ? F[row] : (CT)__ldcg(G + (row - SR)); };
-        auto stv = [&](int row, CT x) {
-            if (!HYB || row < SR) F[row] = x;
-            else __stcg(G + (row - SR), x);
-        };
+        TS w;
+        w.F = F;
+        w.G = G;
+        w.Eg = (const ST *)u.E;
+        w.slice_off = u.slice_off;
+        w.gpeer0 = HYB ? T.gscratch + (long long)(blockIdx.x - rank) * T.gstride : nullptr;
+        w.gstride = T.gstride;
+        w.SR = HYB ? u.srows : rows; /* rows in shared memory */
+        w.s_lo = lo >> 5;
+        w.s_hi = hi >> 5;
+        w.s0 = u.s0;
+        w.n0 = u.n0;
+        w.n1 = u.n1;
+        w.rank = rank;
+        w.C = C;
+        w.pk = (CT)u.p[k];
+        w.mgk = (CT)u.mg[k];
+        w.d = (CT)u.d;
         /* the full replica */
         for (int v = tid; v < rows; v += blockDim.x) {
             CT x;
@@ -459,80 +561,48 @@ __global__ void __launch_bounds__(1024, 1) k_tail(const __grid_constant__ TailPa
                     x = c == (long long)INT64_MAX ? TOPI : (CT)c;
                 }
             }
-            stv(v, x);
+            if (!HYB || v < w.SR) F[v] = x;
+            else __stcg(G + (v - w.SR), x);
         }
-        const CT pk = (CT)u.p[k], mgk = (CT)u.mg[k], d = (CT)u.d;
+        /* the range's slots behind the replica, when they fit (whole
+         * slices: a multiple of 32 slots, 16-byte aligned in both places) */
+        w.b0 = __ldg(u.slice_off + w.s_lo);
+        const int b1 = __ldg(u.slice_off + w.s_hi);
+        const long long rep_bytes = ((long long)w.SR * (long long)sizeof(CT) + 15) & ~15LL;
+        const long long slot_bytes = (long long)(b1 - w.b0) * (long long)sizeof(ST);
+        const bool stage = !HYB && rep_bytes + slot_bytes <= (long long)T.smem_bytes &&
+                           ((uintptr_t)(w.Eg + w.b0) & 15) == 0;
+        w.Es = stage ? (const ST *)(smem_raw + rep_bytes) : nullptr;
+        if (stage) {
+            const uint4 *src = (const uint4 *)(w.Eg + w.b0);
+            uint4 *dst = (uint4 *)(smem_raw + rep_bytes);
+            const int n16 = (int)(slot_bytes >> 4);
+            for (int i = tid; i < n16; i += blockDim.x) dst[i] = __ldg(src + i);
+        }
         if (tid == 0) s_word[0] = s_word[1] = s_word[2] = 0u;
         cl.sync();
         long long r = 0;
         int st = EG_OK;
-        const int s_lo = lo >> 5, s_hi = hi >> 5;
-        for (;;) {
-            unsigned raised = 0;
-            for (int s = s_lo + warp; s < s_hi; s += nwarps) {
-                const int b = __ldg(u.slice_off + s);
-                const int W = (__ldg(u.slice_off + s + 1) - b) >> 5;
-                const bool own1 = s >= u.s0;
-                CT acc = own1 ? Lim<CT>::lo_acc : Lim<CT>::hi_acc;
-                for (int c = 0; c < W; c += UNR) {
-                    ST q[UNR];
-#pragma unroll
-                    for (int x = 0; x < UNR; x++)
-                        if (c + x < W) q[x] = S::load(u.E, b + lane + 32 * (c + x));
-                    CT f[UNR];
-                    int wt[UNR];
-#pragma unroll
-                    for (int x = 0; x < UNR; x++) {
-                        if (c + x < W) {
-                            int sc;
-                            S::dec(q[x], sc, wt[x]);
-                            f[x] = ld(sc);
-                        }
-                    }
-#pragma unroll
-                    for (int x = 0; x < UNR; x++) {
-                        if (c + x < W) {
-                            const CT y = f[x] - (CT)wt[x] * d;
-                            acc = own1 ? (y > acc ? y : acc) : (y < acc ? y : acc);
-                        }
-                    }
-                }
-                const int v = 32 * s + lane;
-                const bool real = own1 ? (v - 32 * u.s0 < u.n1) : (v < u.n0);
-                bool up = false;
-                CT nv = 0;
-                if (real) {
-                    const CT val = acc + pk;
-                    nv = val > mgk ? TOPI : (val > 0 ? val : (CT)0);
-                    if (nv > ld(v)) {
-                        stv(v, nv);
-                        up = true;
-                    }
-                }
-                /* the slice's raised credits go to every peer's replica at
-                 * once (32 consecutive rows: one coalesced store per peer) */
-                if (__any_sync(0xffffffffu, up)) {
-                    raised = 1u;
-                    const CT x = ld(v);
-                    for (int q = 1; q < C; q++) {
-                        const int peer = (rank + q) % C;
-                        if (!HYB || v < SR) *cl.map_shared_rank(F + v, peer) = x;
-                        else __stcg((CT *)(T.gscratch + (long long)(blockIdx.x - rank + peer) * T.gstride) + (v - SR), x);
-                    }
-                }
+        for (int iv = 0;; iv++) {
+            long long ns = kTailSweeps;
+            if (T.max_rounds >= 0) ns = max(1LL, min(ns, T.max_rounds - en.sweeps - r));
+            bool raised = false;
+            for (int it = 0; it < (int)ns; it++) {
+                raised |= w.sweep(cl, lane, warp, nwarps);
+                __syncwarp();
             }
-            const int slot = (int)(r % 3);
+            const int slot = iv % 3;
             if (__syncthreads_or((int)raised) && tid == 0) atomicOr(cl.map_shared_rank(&s_word[slot], 0), 1u);
             if (rank == 0 && tid == 0 && T.timeout_ns && globaltimer_ns() - t0 > T.timeout_ns)
                 atomicOr(&s_word[slot], 1u << 16);
             cl.sync();
             const unsigned word = *cl.map_shared_rank(&s_word[slot], 0);
             if (rank == 0 && tid == 0) {
-                s_word[(r + 2) % 3] = 0u;
-                lifts += (unsigned long long)(u.n0 + u.n1);
-                edges += (unsigned long long)u.m;
+                s_word[(slot + 2) % 3] = 0u;
+                lifts += (unsigned long long)(u.n0 + u.n1) * (unsigned long long)ns;
+                edges += (unsigned long long)u.m * (unsigned long long)ns;
             }
-            r++;
+            r += ns;
             if (!(word & 1u)) break;
             if (word & (1u << 16)) {
                 st = EG_ERR_TIMEOUT;
@@ -548,7 +618,7 @@ __global__ void __launch_bounds__(1024, 1) k_tail(const __grid_constant__ TailPa
         for (int v = lo + tid; v < hi; v += blockDim.x) {
             const int o = __ldg(u.orig + v);
             if (o >= 0) {
-                const CT c = ld(v);
+                const CT c = w.ld(v);
                 u.F[(long long)k * u.n + o] = c >= TOPI ? (long long)INT64_MAX : (long long)c;
                 top += c >= TOPI;
             }
@@ -1192,15 +1262,11 @@ eg_status launch_unit_set(UnitLauncher &L, cudaStream_t main, const UnitSet &S, 
     for (int c = 0; c < kTailClasses; c++) {
         if (S.tail_cap[c] == 0) continue;
         const int slot = kNumVariants + c;
-        /* a tail CTA owns its SM: asking for more than half of an SM's
-         * shared memory keeps a second CTA (of this or another cluster) off
-         * it, which would halve a heavy entry's sweep rate */
-        int sm_smem = 0;
-        if (cudaDeviceGetAttribute(&sm_smem, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev) != cudaSuccess) {
-            cudaGetLastError();
-            sm_smem = 0;
-        }
-        const int tsmem = std::max(S.tail_smem[c], std::min(sm_smem / 2 + 1024, unit_smem_budget(dev)));
+        /* a tail CTA owns its SM: all the shared memory a CTA may have
+         * keeps a second CTA (of this or another cluster) off it, which
+         * would halve a heavy entry's sweep rate, and leaves room behind the
+         * replica for the CTA's slots */
+        const int tsmem = std::max(S.tail_smem[c], unit_smem_budget(dev));
         /* 16-CTA clusters where they can be scheduled, else 8 */
         int csize = kTailCluster;
         int ncl = tail_clusters(c, csize, 1024, tsmem);
@@ -1217,6 +1283,7 @@ eg_status launch_unit_set(UnitLauncher &L, cudaStream_t main, const UnitSet &S, 
         tp.t_start = &ctrl->t_start;
         tp.max_rounds = max_rounds;
         tp.timeout_ns = timeout_ns;
+        tp.smem_bytes = tsmem;
         if (S.tail_gbytes[c] > 0) {
             if (!gs) return eg_set_error(EG_ERR_INVALID, "hybrid tail without scratch");
             ncl = std::min(ncl, tail_hyb_ctas(num_sms) / csize);

@@ -154,6 +154,8 @@ struct TailParams {
     long long gstride;         /* bytes per region                             */
     long long max_rounds;
     unsigned long long timeout_ns;
+    int smem_bytes;            /* dynamic shared memory of the launch          */
+    int pad;
 };
 
 /* Choice of credit width and group size for a game. */
