@@ -123,7 +123,7 @@ def test_round_kinds_give_identical_credits(cfg2_2e14, d, bits):
     else:
         np.testing.assert_array_equal(f, ref)
     assert st.grid > 1  # the grid kernel, not the one-CTA one
-    sweeps = 2  # default sweeps per dense round; dense_rounds counts sweeps
+    sweeps = 4  # default sweeps per dense round; dense_rounds counts sweeps
     if d["direction"] == eg.DIRECTION_SPARSE:
         assert st.dense_rounds == 0
     elif d["direction"] == eg.DIRECTION_DENSE:
