@@ -316,7 +316,7 @@ class Batch:
 
     def __init__(self, games: list[Game], thresholds: int, scale: int = 1, block: int = 0, device: int = 0,
                  max_rounds: int = -1, timeout_ms: float = 0.0, use_graph: bool = False, group_max: int = 0,
-                 tail_rows: int = 0, park_percent: int = 0):
+                 tail_rows: int = 0, park_percent: int = 0, tail_sweeps: int = 0, tail_cluster: int = 0):
         self._h = C.c_void_p()
         self._keep = [g.c_struct() for g in games]
         arr = (_ffi.EgGame * len(games))(*self._keep)
@@ -331,6 +331,8 @@ class Batch:
         o.group_max = group_max
         o.tail_rows = tail_rows
         o.park_percent = park_percent
+        o.tail_sweeps = tail_sweeps
+        o.tail_cluster = tail_cluster
         _check(lib().eg_batch_create(arr, len(games), C.byref(o), C.byref(self._h)))
         self.sizes = [g.num_nodes for g in games]
         self.K = thresholds

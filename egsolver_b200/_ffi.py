@@ -128,7 +128,9 @@ class EgBatchOpts(C.Structure):
         ("group_max", C.c_int32),
         ("tail_rows", C.c_int32),
         ("park_percent", C.c_int32),
-        ("reserved", C.c_int32 * 4),
+        ("tail_sweeps", C.c_int32),
+        ("tail_cluster", C.c_int32),
+        ("reserved", C.c_int32 * 2),
     ]
 
 

@@ -385,9 +385,6 @@ unit_kernel_t kernel_of(int v)
 
 namespace cg = cooperative_groups;
 
-/* Sweeps a CTA runs between two cluster barriers. */
-constexpr int kTailSweeps = 4;
-
 /* Every CTA of the cluster holds a full replica of the unit's credits in
  * its shared memory and lifts the slices of its own row range [rank * R,
  * (rank + 1) * R) (R = ceil(rows / cluster size) rounded up to 32, so a
@@ -398,7 +395,8 @@ constexpr int kTailSweeps = 4;
  * every peer's replica right away (one coalesced store per peer through
  * the cluster's distributed shared memory).
  *
- * A CTA runs up to kTailSweeps sweeps between two cluster barriers, its
+ * A CTA runs T.sweeps sweeps between two cluster barriers (fewer at a
+ * sweep cap), its
  * warps without waiting for one another, and reads whatever its replica
  * holds: every value there is a credit some CTA computed, hence below the
  * least fixed point, so the iteration stays a fair chaotic one.  The
@@ -409,11 +407,11 @@ constexpr int kTailSweeps = 4;
  * gathered in rank 0's shared memory (three rotating words, as in phase 1).
  * Random 4-byte gathers through distributed shared memory are about ten
  * times slower than local ones, hence the replicas. */
-template <typename CT, bool WIDE, bool HYB>
+template <typename CT, bool WIDE>
 struct TailSweep {
     using S = Slot<WIDE>;
     using ST = typename S::T;
-    static constexpr int UNR = sizeof(CT) == 4 ? 4 : 2;
+    static constexpr int UNR = sizeof(CT) == 4 ? 3 : 2; /* spill-free at 64 registers */
     CT *F;             /* the replica (shared memory)                          */
     CT *G;             /* hybrid: rows >= SR of this CTA's replica (global)    */
     const ST *Es;      /* the range's slots in shared memory (staged) or null  */
@@ -426,7 +424,7 @@ struct TailSweep {
 
     __device__ __forceinline__ CT ld(int row) const
     {
-        return (!HYB || row < SR) ? F[row] : (CT)__ldcg(G + (row - SR));
+        return row < SR ? F[row] : (CT)__ldcg(G + (row - SR));
     }
 
     /* One sweep of the warp's slices; true if a credit rose.  Slots are
@@ -471,7 +469,7 @@ struct TailSweep {
                 const CT val = acc + pk;
                 const CT nv = val > mgk ? Lim<CT>::top : (val > 0 ? val : (CT)0);
                 if (nv > ld(v)) {
-                    if (!HYB || v < SR) F[v] = nv;
+                    if (v < SR) F[v] = nv;
                     else __stcg(G + (v - SR), nv);
                     up = true;
                 }
@@ -483,7 +481,7 @@ struct TailSweep {
                 const CT x = ld(v);
                 for (int q = 1; q < C; q++) {
                     const int peer = rank + q < C ? rank + q : rank + q - C;
-                    if (!HYB || v < SR) *cl.map_shared_rank(F + v, peer) = x;
+                    if (v < SR) *cl.map_shared_rank(F + v, peer) = x;
                     else __stcg((CT *)(gpeer0 + (long long)peer * gstride) + (v - SR), x);
                 }
             }
@@ -492,10 +490,10 @@ struct TailSweep {
     }
 };
 
-template <typename CT, bool WIDE, bool HYB>
+template <typename CT, bool WIDE>
 __global__ void __launch_bounds__(1024, 1) k_tail(const __grid_constant__ TailParams T)
 {
-    using TS = TailSweep<CT, WIDE, HYB>;
+    using TS = TailSweep<CT, WIDE>;
     using ST = typename TS::ST;
     constexpr CT TOPI = Lim<CT>::top, LOWI = Lim<CT>::low;
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -506,9 +504,6 @@ __global__ void __launch_bounds__(1024, 1) k_tail(const __grid_constant__ TailPa
     const int rank = (int)cl.block_rank();
     const int C = (int)cl.num_blocks();
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nwarps = blockDim.x >> 5;
-    /* hybrid: rows >= srows of this CTA's replica live in its own global
-     * region, which its peers write (read through L2) */
-    CT *G = HYB ? (CT *)(T.gscratch + (long long)blockIdx.x * T.gstride) : nullptr;
     if (tid == 0) {
         const unsigned long long now = globaltimer_ns();
         atomicCAS(&T.ctrl->t_begin, 0ull, now);
@@ -526,6 +521,10 @@ __global__ void __launch_bounds__(1024, 1) k_tail(const __grid_constant__ TailPa
         const TailEntry en = T.list->e[ei];
         const UnitDesc &u = T.units[en.unit];
         const int k = en.k;
+        const bool hyb = (u.variant & kUnitGlobal) != 0;
+        /* hybrid: rows >= srows of this CTA's replica live in its own
+         * global region, which its peers write (read through L2) */
+        CT *G = hyb ? (CT *)(T.gscratch + (long long)blockIdx.x * T.gstride) : nullptr;
         const int npad = 32 * u.ns, rows = npad + 2;
         const int R = (((rows + C - 1) / C) + 31) & ~31;
         const int lo = min(rows, rank * R);
@@ -535,9 +534,9 @@ __global__ void __launch_bounds__(1024, 1) k_tail(const __grid_constant__ TailPa
         w.G = G;
         w.Eg = (const ST *)u.E;
         w.slice_off = u.slice_off;
-        w.gpeer0 = HYB ? T.gscratch + (long long)(blockIdx.x - rank) * T.gstride : nullptr;
+        w.gpeer0 = hyb ? T.gscratch + (long long)(blockIdx.x - rank) * T.gstride : nullptr;
         w.gstride = T.gstride;
-        w.SR = HYB ? u.srows : rows; /* rows in shared memory */
+        w.SR = hyb ? u.srows : rows; /* rows in shared memory */
         w.s_lo = lo >> 5;
         w.s_hi = hi >> 5;
         w.s0 = u.s0;
@@ -561,7 +560,7 @@ __global__ void __launch_bounds__(1024, 1) k_tail(const __grid_constant__ TailPa
                     x = c == (long long)INT64_MAX ? TOPI : (CT)c;
                 }
             }
-            if (!HYB || v < w.SR) F[v] = x;
+            if (v < w.SR) F[v] = x;
             else __stcg(G + (v - w.SR), x);
         }
         /* the range's slots behind the replica, when they fit (whole
@@ -570,7 +569,7 @@ __global__ void __launch_bounds__(1024, 1) k_tail(const __grid_constant__ TailPa
         const int b1 = __ldg(u.slice_off + w.s_hi);
         const long long rep_bytes = ((long long)w.SR * (long long)sizeof(CT) + 15) & ~15LL;
         const long long slot_bytes = (long long)(b1 - w.b0) * (long long)sizeof(ST);
-        const bool stage = !HYB && rep_bytes + slot_bytes <= (long long)T.smem_bytes &&
+        const bool stage = !hyb && rep_bytes + slot_bytes <= (long long)T.smem_bytes &&
                            ((uintptr_t)(w.Eg + w.b0) & 15) == 0;
         w.Es = stage ? (const ST *)(smem_raw + rep_bytes) : nullptr;
         if (stage) {
@@ -584,7 +583,7 @@ __global__ void __launch_bounds__(1024, 1) k_tail(const __grid_constant__ TailPa
         long long r = 0;
         int st = EG_OK;
         for (int iv = 0;; iv++) {
-            long long ns = kTailSweeps;
+            long long ns = T.sweeps;
             if (T.max_rounds >= 0) ns = max(1LL, min(ns, T.max_rounds - en.sweeps - r));
             bool raised = false;
             for (int it = 0; it < (int)ns; it++) {
@@ -692,14 +691,10 @@ typedef void (*tail_kernel_t)(TailParams);
 tail_kernel_t tail_kernel_of(int cls)
 {
     switch (cls) {
-    case 0: return (tail_kernel_t)k_tail<int, false, false>;
-    case 1: return (tail_kernel_t)k_tail<long long, false, false>;
-    case 2: return (tail_kernel_t)k_tail<int, true, false>;
-    case 3: return (tail_kernel_t)k_tail<long long, true, false>;
-    case 4: return (tail_kernel_t)k_tail<int, false, true>;
-    case 5: return (tail_kernel_t)k_tail<long long, false, true>;
-    case 6: return (tail_kernel_t)k_tail<int, true, true>;
-    default: return (tail_kernel_t)k_tail<long long, true, true>;
+    case 0: return (tail_kernel_t)k_tail<int, false>;
+    case 1: return (tail_kernel_t)k_tail<long long, false>;
+    case 2: return (tail_kernel_t)k_tail<int, true>;
+    default: return (tail_kernel_t)k_tail<long long, true>;
     }
 }
 
@@ -1201,7 +1196,8 @@ static int tail_clusters(int cls, int csize, int block, int smem)
 
 eg_status launch_unit_set(UnitLauncher &L, cudaStream_t main, const UnitSet &S, const UnitDesc *units_dev,
                           TailList *tails, void *tail_scratch, LaunchCtrl *ctrl, int block, int num_sms,
-                          long long max_rounds, unsigned long long timeout_ns, int *grid_total, int park_percent)
+                          long long max_rounds, unsigned long long timeout_ns, int *grid_total, int park_percent,
+                          int tail_sweeps, int tail_cluster)
 {
     cudaError_t e = cudaMemsetAsync(ctrl, 0, sizeof(LaunchCtrl), main);
     if (e != cudaSuccess) return eg_set_error(EG_ERR_CUDA, "launch set-up failed: %s", cudaGetErrorString(e));
@@ -1267,11 +1263,12 @@ eg_status launch_unit_set(UnitLauncher &L, cudaStream_t main, const UnitSet &S, 
          * would halve a heavy entry's sweep rate, and leaves room behind the
          * replica for the CTA's slots */
         const int tsmem = std::max(S.tail_smem[c], unit_smem_budget(dev));
-        /* 16-CTA clusters where they can be scheduled, else 8 */
-        int csize = kTailCluster;
+        /* clusters of tail_cluster CTAs where they can be scheduled, else
+         * half as many, down to 8 */
+        int csize = tail_cluster > 0 ? tail_cluster : kTailCluster;
         int ncl = tail_clusters(c, csize, 1024, tsmem);
-        if (ncl < 1) {
-            csize = 8;
+        while (ncl < 1 && csize > 8) {
+            csize >>= 1;
             ncl = tail_clusters(c, csize, 1024, tsmem);
         }
         if (ncl < 1) return eg_set_error(EG_ERR_CUDA, "tail kernel clusters do not fit (%d B shared)", tsmem);
@@ -1284,6 +1281,7 @@ eg_status launch_unit_set(UnitLauncher &L, cudaStream_t main, const UnitSet &S, 
         tp.max_rounds = max_rounds;
         tp.timeout_ns = timeout_ns;
         tp.smem_bytes = tsmem;
+        tp.sweeps = std::max(1, tail_sweeps);
         if (S.tail_gbytes[c] > 0) {
             if (!gs) return eg_set_error(EG_ERR_INVALID, "hybrid tail without scratch");
             ncl = std::min(ncl, tail_hyb_ctas(num_sms) / csize);
@@ -1341,6 +1339,8 @@ struct eg_batch {
     int num_games = 0, K = 0, d = 1;
     long long total_nodes = 0, total_edges = 0;
     int block = 1024, kg_cap = 8, smem_budget = 0, sms = 148, tail_rows = 0, park_percent = 10;
+    int tail_sweeps = kTailSweeps;
+    int tail_cluster = kTailCluster;
     long long max_rounds = -1;
     double timeout_ms = 0;
     std::vector<HostPacked> hp;      /* host images (slots dropped after upload) */
@@ -1460,6 +1460,11 @@ extern "C" eg_status eg_batch_create(const eg_game *games, int32_t num_games, co
         return eg_set_error(EG_ERR_INVALID, "block must be a multiple of 32 in [64, 1024]");
     if (opts->group_max && opts->group_max != 1 && opts->group_max != 2 && opts->group_max != 4 && opts->group_max != 8)
         return eg_set_error(EG_ERR_INVALID, "group_max must be 1, 2, 4 or 8");
+    if (opts->tail_sweeps < 0 || opts->tail_sweeps > 16)
+        return eg_set_error(EG_ERR_INVALID, "tail_sweeps must be in [0, 16]");
+    if (opts->tail_cluster != 0 && opts->tail_cluster != 1 && opts->tail_cluster != 2 && opts->tail_cluster != 4 &&
+        opts->tail_cluster != 8 && opts->tail_cluster != 16)
+        return eg_set_error(EG_ERR_INVALID, "tail_cluster must be 0, 1, 2, 4, 8 or 16");
     long long tn = 0, tm = 0;
     for (int g = 0; g < num_games; g++) {
         eg_status s = eg_validate(&games[g]);
@@ -1488,6 +1493,8 @@ extern "C" eg_status eg_batch_create(const eg_game *games, int32_t num_games, co
     b->kg_cap = opts->group_max ? opts->group_max : 8;
     b->tail_rows = opts->tail_rows > 0 ? opts->tail_rows : 0;
     b->park_percent = opts->park_percent > 0 ? opts->park_percent : 10;
+    b->tail_sweeps = opts->tail_sweeps > 0 ? opts->tail_sweeps : kTailSweeps;
+    b->tail_cluster = opts->tail_cluster > 0 ? opts->tail_cluster : kTailCluster;
     b->max_rounds = opts->max_rounds;
     b->timeout_ms = opts->timeout_ms;
     b->use_graph = opts->use_graph != 0;
@@ -1667,7 +1674,7 @@ static eg_status batch_enqueue(eg_batch *b, cudaStream_t st, int *grid)
 {
     const unsigned long long tns = b->timeout_ms > 0 ? (unsigned long long)(b->timeout_ms * 1e6) : 0ull;
     return launch_unit_set(b->launcher, st, b->set, b->units_dev, (TailList *)b->tails, b->tscratch, b->ctrl, b->block,
-                           b->sms, b->max_rounds, tns, grid, b->park_percent);
+                           b->sms, b->max_rounds, tns, grid, b->park_percent, b->tail_sweeps, b->tail_cluster);
 }
 
 extern "C" eg_status eg_batch_solve(eg_batch *b, eg_batch_stats *stats)

@@ -108,10 +108,12 @@ struct UnitCtrl {
  * (credit width x slot width).  Entries come from units too large for one
  * CTA (listed by the host, solved from 0) and from units that phase 1 parks
  * when the GPU runs out of other work (resumed from their credits). */
-/* tail classes: (64-bit credits ? 1 : 0) | (8-byte slots ? 2 : 0) | (hybrid ? 4 : 0);
- * a hybrid unit keeps rows >= srows in global memory (each cluster CTA its
- * own copy there) */
-constexpr int kTailClasses = 8;
+/* tail classes: (64-bit credits ? 1 : 0) | (8-byte slots ? 2 : 0), one
+ * kernel each; a hybrid unit (rows >= srows in global memory, each cluster
+ * CTA its own copy there) runs in its class's kernel, which tells it apart
+ * at run time */
+constexpr int kTailClasses = 4;
+constexpr int kTailSweeps = 1;   /* default sweeps between two cluster barriers */
 constexpr int kTailCluster = 16; /* CTAs per cluster (8 where 16 cannot be scheduled) */
 struct TailEntry {
     int unit;                  /* index into the unit array                   */
@@ -128,7 +130,7 @@ struct TailList {
 };
 __host__ __device__ inline int tail_class(int variant)
 {
-    return ((variant & kUnitCredit64) ? 1 : 0) | ((variant & kUnitWide) ? 2 : 0) | ((variant & kUnitGlobal) ? 4 : 0);
+    return ((variant & kUnitCredit64) ? 1 : 0) | ((variant & kUnitWide) ? 2 : 0);
 }
 
 struct UnitParams {
@@ -155,7 +157,7 @@ struct TailParams {
     long long max_rounds;
     unsigned long long timeout_ns;
     int smem_bytes;            /* dynamic shared memory of the launch          */
-    int pad;
+    int sweeps;                /* sweeps between two cluster barriers          */
 };
 
 /* Choice of credit width and group size for a game. */
@@ -245,7 +247,8 @@ struct LaunchCtrl {
 eg_status launch_unit_set(UnitLauncher &L, cudaStream_t main, const UnitSet &S, const UnitDesc *units_dev,
                           TailList *tails, void *tail_scratch, LaunchCtrl *ctrl, int block, int num_sms,
                           long long max_rounds, unsigned long long timeout_ns, int *grid_total,
-                          int park_percent = 10);
+                          int park_percent = 10, int tail_sweeps = kTailSweeps,
+                          int tail_cluster = kTailCluster);
 /* Totals of the per-variant and per-tail-class counters. */
 void sum_ctrl(const LaunchCtrl &c, UnitCtrl *out);
 

@@ -459,7 +459,7 @@ bool launch_ready(eg_server *s)
         ls = launch_unit_set(s->launchers[(size_t)l.stream], st, S, l.dunits, tl, l.dscratch, l.dctrl, s->o.block,
                              s->sms, s->o.max_rounds, 0, &grid);
         if (ls == EG_OK) e = cudaEventRecord(l.ev, st);
-        /* the tail lists' host image is copied from pageable memory: wait for
+        /* the tail list's host image is copied from pageable memory: wait for
          * the copy before S goes out of scope */
         if (ls == EG_OK && e == cudaSuccess) e = cudaStreamSynchronize(s->upload_stream);
     }
