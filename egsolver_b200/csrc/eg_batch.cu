@@ -407,11 +407,11 @@ namespace cg = cooperative_groups;
  * gathered in rank 0's shared memory (three rotating words, as in phase 1).
  * Random 4-byte gathers through distributed shared memory are about ten
  * times slower than local ones, hence the replicas. */
-template <typename CT, bool WIDE>
+template <typename CT, bool WIDE, bool HYB>
 struct TailSweep {
     using S = Slot<WIDE>;
     using ST = typename S::T;
-    static constexpr int UNR = sizeof(CT) == 4 ? 3 : 2; /* spill-free at 64 registers */
+    static constexpr int UNR = sizeof(CT) == 4 ? 4 : 2;
     CT *F;             /* the replica (shared memory)                          */
     CT *G;             /* hybrid: rows >= SR of this CTA's replica (global)    */
     const ST *Es;      /* the range's slots in shared memory (staged) or null  */
@@ -424,7 +424,7 @@ struct TailSweep {
 
     __device__ __forceinline__ CT ld(int row) const
     {
-        return row < SR ? F[row] : (CT)__ldcg(G + (row - SR));
+        return (!HYB || row < SR) ? F[row] : (CT)__ldcg(G + (row - SR));
     }
 
     /* One sweep of the warp's slices; true if a credit rose.  Slots are
@@ -469,7 +469,7 @@ struct TailSweep {
                 const CT val = acc + pk;
                 const CT nv = val > mgk ? Lim<CT>::top : (val > 0 ? val : (CT)0);
                 if (nv > ld(v)) {
-                    if (v < SR) F[v] = nv;
+                    if (!HYB || v < SR) F[v] = nv;
                     else __stcg(G + (v - SR), nv);
                     up = true;
                 }
@@ -481,7 +481,7 @@ struct TailSweep {
                 const CT x = ld(v);
                 for (int q = 1; q < C; q++) {
                     const int peer = rank + q < C ? rank + q : rank + q - C;
-                    if (v < SR) *cl.map_shared_rank(F + v, peer) = x;
+                    if (!HYB || v < SR) *cl.map_shared_rank(F + v, peer) = x;
                     else __stcg((CT *)(gpeer0 + (long long)peer * gstride) + (v - SR), x);
                 }
             }
@@ -490,10 +490,10 @@ struct TailSweep {
     }
 };
 
-template <typename CT, bool WIDE>
+template <typename CT, bool WIDE, bool HYB>
 __global__ void __launch_bounds__(1024, 1) k_tail(const __grid_constant__ TailParams T)
 {
-    using TS = TailSweep<CT, WIDE>;
+    using TS = TailSweep<CT, WIDE, HYB>;
     using ST = typename TS::ST;
     constexpr CT TOPI = Lim<CT>::top, LOWI = Lim<CT>::low;
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -504,6 +504,9 @@ __global__ void __launch_bounds__(1024, 1) k_tail(const __grid_constant__ TailPa
     const int rank = (int)cl.block_rank();
     const int C = (int)cl.num_blocks();
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nwarps = blockDim.x >> 5;
+    /* hybrid: rows >= srows of this CTA's replica live in its own global
+     * region, which its peers write (read through L2) */
+    CT *G = HYB ? (CT *)(T.gscratch + (long long)blockIdx.x * T.gstride) : nullptr;
     if (tid == 0) {
         const unsigned long long now = globaltimer_ns();
         atomicCAS(&T.ctrl->t_begin, 0ull, now);
@@ -521,10 +524,6 @@ __global__ void __launch_bounds__(1024, 1) k_tail(const __grid_constant__ TailPa
         const TailEntry en = T.list->e[ei];
         const UnitDesc &u = T.units[en.unit];
         const int k = en.k;
-        const bool hyb = (u.variant & kUnitGlobal) != 0;
-        /* hybrid: rows >= srows of this CTA's replica live in its own
-         * global region, which its peers write (read through L2) */
-        CT *G = hyb ? (CT *)(T.gscratch + (long long)blockIdx.x * T.gstride) : nullptr;
         const int npad = 32 * u.ns, rows = npad + 2;
         const int R = (((rows + C - 1) / C) + 31) & ~31;
         const int lo = min(rows, rank * R);
@@ -534,9 +533,9 @@ __global__ void __launch_bounds__(1024, 1) k_tail(const __grid_constant__ TailPa
         w.G = G;
         w.Eg = (const ST *)u.E;
         w.slice_off = u.slice_off;
-        w.gpeer0 = hyb ? T.gscratch + (long long)(blockIdx.x - rank) * T.gstride : nullptr;
+        w.gpeer0 = HYB ? T.gscratch + (long long)(blockIdx.x - rank) * T.gstride : nullptr;
         w.gstride = T.gstride;
-        w.SR = hyb ? u.srows : rows; /* rows in shared memory */
+        w.SR = HYB ? u.srows : rows; /* rows in shared memory */
         w.s_lo = lo >> 5;
         w.s_hi = hi >> 5;
         w.s0 = u.s0;
@@ -560,7 +559,7 @@ __global__ void __launch_bounds__(1024, 1) k_tail(const __grid_constant__ TailPa
                     x = c == (long long)INT64_MAX ? TOPI : (CT)c;
                 }
             }
-            if (v < w.SR) F[v] = x;
+            if (!HYB || v < w.SR) F[v] = x;
             else __stcg(G + (v - w.SR), x);
         }
         /* the range's slots behind the replica, when they fit (whole
@@ -569,7 +568,7 @@ __global__ void __launch_bounds__(1024, 1) k_tail(const __grid_constant__ TailPa
         const int b1 = __ldg(u.slice_off + w.s_hi);
         const long long rep_bytes = ((long long)w.SR * (long long)sizeof(CT) + 15) & ~15LL;
         const long long slot_bytes = (long long)(b1 - w.b0) * (long long)sizeof(ST);
-        const bool stage = !hyb && rep_bytes + slot_bytes <= (long long)T.smem_bytes &&
+        const bool stage = !HYB && rep_bytes + slot_bytes <= (long long)T.smem_bytes &&
                            ((uintptr_t)(w.Eg + w.b0) & 15) == 0;
         w.Es = stage ? (const ST *)(smem_raw + rep_bytes) : nullptr;
         if (stage) {
@@ -691,10 +690,14 @@ typedef void (*tail_kernel_t)(TailParams);
 tail_kernel_t tail_kernel_of(int cls)
 {
     switch (cls) {
-    case 0: return (tail_kernel_t)k_tail<int, false>;
-    case 1: return (tail_kernel_t)k_tail<long long, false>;
-    case 2: return (tail_kernel_t)k_tail<int, true>;
-    default: return (tail_kernel_t)k_tail<long long, true>;
+    case 0: return (tail_kernel_t)k_tail<int, false, false>;
+    case 1: return (tail_kernel_t)k_tail<long long, false, false>;
+    case 2: return (tail_kernel_t)k_tail<int, true, false>;
+    case 3: return (tail_kernel_t)k_tail<long long, true, false>;
+    case 4: return (tail_kernel_t)k_tail<int, false, true>;
+    case 5: return (tail_kernel_t)k_tail<long long, false, true>;
+    case 6: return (tail_kernel_t)k_tail<int, true, true>;
+    default: return (tail_kernel_t)k_tail<long long, true, true>;
     }
 }
 

@@ -108,12 +108,11 @@ struct UnitCtrl {
  * (credit width x slot width).  Entries come from units too large for one
  * CTA (listed by the host, solved from 0) and from units that phase 1 parks
  * when the GPU runs out of other work (resumed from their credits). */
-/* tail classes: (64-bit credits ? 1 : 0) | (8-byte slots ? 2 : 0), one
- * kernel each; a hybrid unit (rows >= srows in global memory, each cluster
- * CTA its own copy there) runs in its class's kernel, which tells it apart
- * at run time */
-constexpr int kTailClasses = 4;
-constexpr int kTailSweeps = 1;   /* default sweeps between two cluster barriers */
+/* tail classes: (64-bit credits ? 1 : 0) | (8-byte slots ? 2 : 0) | (hybrid ? 4 : 0);
+ * a hybrid unit keeps rows >= srows in global memory (each cluster CTA its
+ * own copy there) */
+constexpr int kTailClasses = 8;
+constexpr int kTailSweeps = 4;   /* default sweeps between two cluster barriers */
 constexpr int kTailCluster = 16; /* CTAs per cluster (8 where 16 cannot be scheduled) */
 struct TailEntry {
     int unit;                  /* index into the unit array                   */
@@ -130,7 +129,7 @@ struct TailList {
 };
 __host__ __device__ inline int tail_class(int variant)
 {
-    return ((variant & kUnitCredit64) ? 1 : 0) | ((variant & kUnitWide) ? 2 : 0);
+    return ((variant & kUnitCredit64) ? 1 : 0) | ((variant & kUnitWide) ? 2 : 0) | ((variant & kUnitGlobal) ? 4 : 0);
 }
 
 struct UnitParams {

@@ -295,7 +295,7 @@ typedef struct eg_batch_opts {
                                     share of phase-1 CTAs is idle (0: 10; above 100:
                                     never)                                          */
     int32_t tail_sweeps;         /* sweeps a cluster CTA runs between two cluster
-                                    barriers in the tail, 1..16 (0: 1)              */
+                                    barriers in the tail, 1..16 (0: 4)              */
     int32_t tail_cluster;        /* CTAs per tail cluster: 1, 2, 4, 8 or 16 (0: 16;
                                     halved down to 8 where it cannot be scheduled) */
     int32_t reserved[2];
