@@ -91,7 +91,9 @@ def parse():
     ap.add_argument("--variant", type=int, default=0)
     ap.add_argument("--narrow", action="store_true", help="allow 32-bit device credits where exact")
     ap.add_argument("--tune", action="store_true",
-                    help="autotune the layout and dense-round knobs (eg_dgame_tune) before the timed steps")
+                    help="autotune the layout and dense-round knobs (eg_dgame_tune) before the timed steps "
+                         "(the default for single-game workloads without --variant or --max-rounds)")
+    ap.add_argument("--no-tune", action="store_true", help="time the solver's default knobs")
     ap.add_argument("--case", choices=["frontier-sparse60", "units-small24", "tail-game26"], default=None,
                     help="profiling case: one small, fixed launch of a kernel for ncu (prints a labelled line, "
                          "not a benchmark)")
@@ -631,7 +633,9 @@ def main():
               narrow=args.narrow)
     capped = args.max_rounds >= 0
     tuned = None
-    if args.tune:
+    # the autotuner is part of the solver: it runs once per game, outside
+    # the timed region, and the line reports the knobs it chose
+    if args.tune or (not args.no_tune and not args.variant and not capped):
         knobs, rep = res.tune(rounds=300, **kw)
         kw.update(knobs)
         tuned = {"knobs": knobs, **rep}

@@ -1258,7 +1258,16 @@ eg_status launch_unit_set(UnitLauncher &L, cudaStream_t main, const UnitSet &S, 
     char *gs = (char *)tail_scratch;
     int dev = 0;
     cudaGetDevice(&dev);
-    for (int c = 0; c < kTailClasses; c++) {
+    /* the class kernels share the GPU, and whichever's clusters start first
+     * hold their SMs until its list is empty; hybrid classes (rows in
+     * global memory, the slowest sweeps, so the likeliest to bound the
+     * tail) launch first and at the greatest priority */
+    int prio_least = 0, prio_greatest = 0;
+    if (cudaDeviceGetStreamPriorityRange(&prio_least, &prio_greatest) != cudaSuccess) {
+        cudaGetLastError();
+        prio_least = prio_greatest = 0;
+    }
+    for (int c = kTailClasses - 1; c >= 0; c--) {
         if (S.tail_cap[c] == 0) continue;
         const int slot = kNumVariants + c;
         /* a tail CTA owns its SM: all the shared memory a CTA may have
@@ -1294,20 +1303,29 @@ eg_status launch_unit_set(UnitLauncher &L, cudaStream_t main, const UnitSet &S, 
         }
         cudaLaunchConfig_t cfg;
         memset(&cfg, 0, sizeof cfg);
-        cudaLaunchAttribute attr[1];
+        cudaLaunchAttribute attr[2];
         attr[0].id = cudaLaunchAttributeClusterDimension;
         attr[0].val.clusterDim.x = csize;
         attr[0].val.clusterDim.y = 1;
         attr[0].val.clusterDim.z = 1;
+        attr[1].id = cudaLaunchAttributePriority;
+        attr[1].val.priority = (c & 4) ? prio_greatest : prio_least;
         const int ent = S.tail_cap[c];
         cfg.gridDim = dim3(csize * std::max(1, std::min(ncl, ent)));
         cfg.blockDim = dim3(1024);
         cfg.dynamicSmemBytes = (size_t)tsmem;
         cfg.stream = L.aux[slot];
         cfg.attrs = attr;
-        cfg.numAttrs = 1;
+        cfg.numAttrs = 2;
         e = cudaStreamWaitEvent(L.aux[slot], L.fork2, 0);
-        if (e == cudaSuccess) e = cudaLaunchKernelEx(&cfg, tail_kernel_of(c), tp);
+        if (e == cudaSuccess) {
+            e = cudaLaunchKernelEx(&cfg, tail_kernel_of(c), tp);
+            if (e != cudaSuccess) { /* without the priority, where it is refused */
+                cudaGetLastError();
+                cfg.numAttrs = 1;
+                e = cudaLaunchKernelEx(&cfg, tail_kernel_of(c), tp);
+            }
+        }
         if (e == cudaSuccess) e = cudaEventRecord(L.join[slot], L.aux[slot]);
         if (e == cudaSuccess) e = cudaStreamWaitEvent(main, L.join[slot], 0);
         if (e != cudaSuccess) return eg_set_error(EG_ERR_CUDA, "tail kernel launch failed: %s", cudaGetErrorString(e));
