@@ -135,3 +135,12 @@ def test_bad_options_rejected_before_any_device_work():
         with pytest.raises(eg.EGError) as ei:
             eg.solve(g, **bad)
         assert ei.value.name == "EG_ERR_INVALID"
+
+
+def test_bad_batch_options_rejected_before_any_device_work():
+    games = [workloads.cfg1()]
+    for bad in (dict(group_max=3), dict(tail_sweeps=17), dict(tail_sweeps=-1), dict(tail_cluster=3),
+                dict(tail_cluster=32), dict(block=48)):
+        with pytest.raises(eg.EGError) as ei:
+            eg.Batch(games, thresholds=2, scale=1, **bad)
+        assert ei.value.name == "EG_ERR_INVALID"

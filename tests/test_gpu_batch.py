@@ -171,3 +171,18 @@ def test_cfg4_game_near_the_top_of_the_size_range():
     for k in (0, 2):
         want, _ = O.eg_solve(eg.threshold_game(g, int(p_all[34, k]), d), bits=64)
         np.testing.assert_array_equal(got[k], want)
+
+
+@pytest.mark.parametrize("tail_sweeps,tail_cluster", [(1, 16), (4, 8), (2, 2)])
+def test_tail_shapes_give_identical_credits(tail_sweeps, tail_cluster):
+    """Every (game, threshold) straight to the cluster tail, at several
+    sweeps per cluster barrier and cluster sizes (CTAs past the rows of a
+    small game hold empty ranges)."""
+    games = small_batch(6, seed=41)
+    p = np.random.default_rng(7).integers(-50, 51, size=(len(games), 4)).astype(np.int32)
+    with eg.Batch(games, thresholds=4, scale=2, tail_rows=1, tail_sweeps=tail_sweeps,
+                  tail_cluster=tail_cluster) as b:
+        b.set_thresholds(p)
+        _, st = b.solve()
+        assert st.games_failed == 0 and st.tail_entries == len(games) * 4
+        check_batch(b, games, p, 2)
