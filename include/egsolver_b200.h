@@ -273,7 +273,10 @@ eg_status eg_csr2csc_i32(int32_t num_rows, int32_t num_cols, int64_t nnz,
  * layout; one persistent launch then solves every (game, threshold) pair.
  * The work is cut into units of one game at a group of 1, 2, 4 or 8
  * thresholds, one CTA per unit with the unit's credits in shared memory,
- * taken from a device queue heaviest first. */
+ * taken from a device queue heaviest first.  When the queue runs dry, the
+ * units still running hand their open thresholds to a cluster tail: each
+ * (game, threshold) on a thread-block cluster whose CTAs each hold a
+ * replica of its credits. */
 #define EG_BATCH_MAX_K 32
 
 typedef struct eg_batch eg_batch;
